@@ -1,0 +1,414 @@
+"""Benchmark of the on-node SpGEMM path (one JSON line on rank 0).
+
+Default workload: plain C = A·A on an R-MAT graph, scale 20 (1,048,576 rows),
+edge factor 16, (a, b, c, d) = (.57, .19, .19, .05), duplicates merged,
+self-loops kept, FP64 values uniform in [-1, 1], int32 CSR in, int64 row
+offsets out (nnz(C) > 2^31).  One step = one full two-phase SpGEMM through
+the C ABI (flop count, symbolic, scan, numeric) into preallocated C.
+
+  value   GFLOP/s = 2 * mults / device time per step, inputs resident in HBM
+  e2e     the same metric with host buffers: pinned host A -> device, the
+          SpGEMM, and C back to pinned host memory inside the timed region
+  roofline  the dominant persistent kernel (symbolic or numeric phase) timed
+          with CUDA events the library records on the call's stream; its
+          algorithmic bytes are bytes(A) + bytes(B) + bytes(C) with
+          bytes(X) = (rows+1)*s + 12*nnz(X)
+  cpu_baseline  the CPU restatement (oracle) on a strided row sample, all host
+          threads
+
+Multi-GPU: every rank runs its own replica of the product ("replicas only";
+the plain product has no exchange step), value = sum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 2**20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="rmat", choices=["rmat", "uniform"])
+    p.add_argument("--scale", type=int, default=20)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def csr_bytes(rows, nnz, s):
+    return (rows + 1) * s + 12 * nnz
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                smax = float(f[2].split()[0])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        busy = [x for x in sm if x > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workload
+def make_workload(args):
+    from trident_b200 import workloads
+    if args.workload == "rmat":
+        A = workloads.rmat(scale=args.scale, edge_factor=args.edge_factor, seed=args.seed)
+        cfg = {"workload": f"rmat{args.scale}_AxA", "rows": A.nrows, "nnz_A": A.nnz,
+               "edge_factor": args.edge_factor, "abcd": [0.57, 0.19, 0.19, 0.05], "seed": args.seed}
+    else:
+        A = workloads.uniform_rows(1024, 16, True, seed=args.seed)
+        cfg = {"workload": "uniform1024_AxA", "rows": A.nrows, "nnz_A": A.nnz, "seed": args.seed}
+    return A, cfg
+
+
+def cpu_baseline(A, mults_total, seconds):
+    """Oracle (CPU restatement, all host threads) on a strided row sample."""
+    import numpy as np
+
+    import oracle
+    from trident_b200.csr import HostCSR
+    rm = oracle.row_mults(A, A)
+    # calibrate: time a small sample, then size the real one to ~`seconds`
+    def sample(stride, offset=0):
+        rows = np.arange(offset, A.nrows, stride)
+        rp = np.zeros(rows.size + 1, dtype=np.int64)
+        rp[1:] = np.cumsum(A.rowptr[rows + 1] - A.rowptr[rows])
+        idx = np.concatenate([np.arange(A.rowptr[r], A.rowptr[r + 1]) for r in rows]) if rows.size else \
+            np.zeros(0, np.int64)
+        return HostCSR(rows.size, A.ncols, rp, A.col[idx], A.val[idx]), int(rm[rows].sum())
+
+    stride = max(1, int(2 ** math.ceil(math.log2(max(1.0, mults_total / 2e8)))))
+    S, mu = sample(stride)
+    t0 = time.perf_counter()
+    oracle.spgemm(S, A, with_abs=False)
+    dt = time.perf_counter() - t0
+    rate = mu / max(dt, 1e-6)
+    want = rate * seconds
+    stride2 = max(1, int(round(mults_total / max(want, 1.0))))
+    S, mu = sample(stride2, offset=1)
+    t0 = time.perf_counter()
+    oracle.spgemm(S, A, with_abs=False)
+    dt = time.perf_counter() - t0
+    return {"value": round(2 * mu / dt / 1e9, 4), "unit": "GFLOP/s", "cores": oracle.num_threads(),
+            "kind": "port",
+            "sample": f"rows i = 1 mod {stride2} of A times A ({S.nrows} rows, {mu} mults, {dt:.1f} s)"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from trident_b200 import ops
+    from trident_b200._lib import TSPG_F_B_SORTED, TspgCsrOut, check, lib
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    A, cfg = make_workload(args)
+    ctx = ops.Context(dev)
+    dA = A.to_device(rowptr_bits=32)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    a = dA.abi()
+    mults, upper = ops.spgemm_count(ctx, dA, dA)
+    plan = ops.Plan(ctx, dA, dA)
+    nnz_c = plan.c_nnz
+    plan.close()
+    rp_bits = 64 if nnz_c > 2**31 - 1 else 32
+    Crp = torch.empty(A.nrows + 1, dtype=torch.int64 if rp_bits == 64 else torch.int32, device="cuda")
+    Ccol = torch.empty(max(nnz_c, 1), dtype=torch.int32, device="cuda")
+    Cval = torch.empty(max(nnz_c, 1), dtype=torch.float64, device="cuda")
+
+    def out():
+        o = TspgCsrOut()
+        o.nrows, o.ncols = A.nrows, A.ncols
+        o.rowptr, o.rowptr_bits, o.val_bits = Crp.data_ptr(), rp_bits, 64
+        o.col, o.val, o.capacity = Ccol.data_ptr(), Cval.data_ptr(), nnz_c
+        return o
+
+    def step():
+        o = out()
+        check(lib.tspg_spgemm(ctx.h, sp, C.byref(a), C.byref(a), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    check(lib.tspg_ctx_phase_timing(ctx.h, 1), "phase timing")
+    launches0 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(launches0))
+    sym_ms, num_ms = [], []
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fs, fn = C.c_float(), C.c_float()
+    for _ in range(args.steps):
+        step()
+        lib.tspg_ctx_phase_ms(ctx.h, C.byref(fs), C.byref(fn))
+        sym_ms.append(fs.value)
+        num_ms.append(fn.value)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    check(lib.tspg_ctx_phase_timing(ctx.h, 0), "phase timing")
+    launches1 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(launches1))
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    flops = 2.0 * mults
+    value = flops / (ms * 1e-3) / 1e9 * world
+
+    # roofline of the dominant persistent kernel
+    bytes_a = csr_bytes(A.nrows, A.nnz, 4)
+    bytes_c = csr_bytes(A.nrows, nnz_c, rp_bits // 8)
+    algo = 2 * bytes_a + bytes_c
+    sym, num = statistics.mean(sym_ms), statistics.mean(num_ms)
+    dom_ms, dom_name = (num, "k_phase<numeric>") if num >= sym else (sym, "k_phase<symbolic>")
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = algo / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        ent = prof.get(cfg["workload"], {}).get(dom_name)
+        if ent:
+            traffic = int(ent["dram_bytes_per_launch"])
+    except Exception:
+        pass
+
+    # e2e through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, (Crp, Ccol, Cval))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(A, mults, args.cpu_seconds)
+
+    line = {
+        "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64",
+        "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
+        "config": dict(cfg, mults=mults, nnz_C=nnz_c, c_rowptr_bits=rp_bits, parallelism=f"replicas{world}",
+                       l2="inputs and outputs larger than L2 (A %.0f MB, C %.0f MB)" % (bytes_a / 1e6, bytes_c / 1e6)),
+        "phase_ms": {"symbolic": round(sym, 3), "numeric": round(num, 3)},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes": algo,
+                     "step_frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4)},
+        "gpu_launches": int(launches1.value - launches0.value),
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    ctx.close()
+    return line
+
+
+def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
+    """Host A (pinned) -> device, SpGEMM through the ABI, C -> pinned host."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from trident_b200._lib import TSPG_F_B_SORTED, TspgCsr, TspgCsrOut, check, lib
+
+    hrp = torch.from_numpy(A.rowptr.astype(np.int32)).pin_memory()
+    hcol = torch.from_numpy(A.col).pin_memory()
+    hval = torch.from_numpy(A.val).pin_memory()
+    drp, dcol, dval = torch.empty_like(hrp, device="cuda"), torch.empty_like(hcol, device="cuda"), \
+        torch.empty_like(hval, device="cuda")
+    # C lands in pinned host memory; when that does not fit, it is streamed
+    # through a pinned staging ring (every byte still crosses to the host)
+    c_bytes = nnz_c * 12 + (A.nrows + 1) * (rp_bits // 8)
+    try:
+        avail = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
+    except Exception:
+        avail = 0
+    full = c_bytes < 0.5 * avail
+    rdt = torch.int64 if rp_bits == 64 else torch.int32
+    Crp, Ccol, Cval = cbufs
+    if full:
+        hC = (torch.empty(Crp.numel(), dtype=rdt, pin_memory=True),
+              torch.empty(Ccol.numel(), dtype=torch.int32, pin_memory=True),
+              torch.empty(Cval.numel(), dtype=torch.float64, pin_memory=True))
+    else:
+        ring = 1 << 30
+        hC = torch.empty(ring, dtype=torch.uint8, pin_memory=True)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def d2h_ring(t):
+        flat = t.view(torch.uint8)
+        for o in range(0, flat.numel(), hC.numel()):
+            n = min(hC.numel(), flat.numel() - o)
+            hC[:n].copy_(flat[o:o + n], non_blocking=True)
+
+    def step():
+        drp.copy_(hrp, non_blocking=True)
+        dcol.copy_(hcol, non_blocking=True)
+        dval.copy_(hval, non_blocking=True)
+        a = TspgCsr(A.nrows, A.ncols, A.nnz, drp.data_ptr(), 32, 64, dcol.data_ptr(), dval.data_ptr())
+        o = TspgCsrOut()
+        o.nrows, o.ncols = A.nrows, A.ncols
+        o.rowptr, o.rowptr_bits, o.val_bits = Crp.data_ptr(), rp_bits, 64
+        o.col, o.val, o.capacity = Ccol.data_ptr(), Cval.data_ptr(), nnz_c
+        check(lib.tspg_spgemm(ctx.h, sp, C.byref(a), C.byref(a), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
+        if full:
+            hC[0].copy_(Crp, non_blocking=True)
+            hC[1].copy_(Ccol[:nnz_c], non_blocking=True)
+            hC[2].copy_(Cval[:nnz_c], non_blocking=True)
+        else:
+            d2h_ring(Crp)
+            d2h_ring(Ccol[:nnz_c])
+            d2h_ring(Cval[:nnz_c])
+
+    steps = max(1, min(args.steps, 3))
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    h2d = (hrp.numel() * 4 + hcol.numel() * 4 + hval.numel() * 8)
+    return {"value": round(2.0 * mults / (ms * 1e-3) / 1e9 * world, 3), "unit": "GFLOP/s",
+            "ms_per_step": round(ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(c_bytes),
+            "c_to_host": "pinned result arrays" if full else "pinned 1 GiB staging ring (host RAM < 2x C)",
+            "steps": steps}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The reference's CPU path for the same product: the oracle restatement
+    of KokkosKernels SpGEMM semantics (KokkosKernels itself is not vendored
+    and cannot be built here), all host threads, bounded row samples."""
+    import time as _t
+
+    import oracle
+    A, cfg = make_workload(args)
+    rm = oracle.row_mults(A, A)
+    mults = int(rm.sum())
+    vals = []
+    per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(A, mults, per)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.mean(x["value"] for x in vals)
+    return {"impl": "reference", "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64", "value": round(v, 4),
+            "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
+            "config": dict(cfg, mults=mults),
+            "cpu_baseline": {"value": round(v, 4), "unit": "GFLOP/s", "cores": vals[-1]["cores"], "kind": "port",
+                             "sample": vals[-1]["sample"]},
+            "e2e": {"value": round(v, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_ours(args, rank, world)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,286 @@
+/*
+ * tspg.h — C ABI of the B200 (sm_100a) on-node SpGEMM path for Trident.
+ *
+ * The library replaces the three library-backed pieces of Trident's per-stage
+ * local compute:
+ *   - the local tile SpGEMM  C = A·B  and the accumulate form  C = C + A·B
+ *     (KokkosSparse::spgemm in include/KokkosWrap.hpp:331,375, and the
+ *      cusparseSpGEMM* paths in include/cusparse_helpers.cuh:908-1344);
+ *   - the merge of partial C tiles  C = A + B  with the union pattern
+ *     (KokkosSparse::spadd_* in include/KokkosWrap.hpp:343-349,420-425 and
+ *      cusparseScsrgeam2* in include/cusparse_helpers.cuh:799-905);
+ *   - the bitmask tile pack / unpack of the sparsity-aware exchange
+ *     (SpaComm::gen_bitmask, intersect_bitmasks, select_entries_cuda,
+ *      select_ptrs and SpaCommHandler::Compress in include/spacomm.cuh:29-148,
+ *      556-623, 808-889, 962-1091).
+ *
+ * Conventions
+ *   - All matrix pointers are DEVICE pointers, 0-based CSR (or CSC where a
+ *     function says so).  Column indices are int32.  Row offsets are int32 or
+ *     int64 (rowptr_bits 32|64).  Values are FP64 (val_bits 64, the graded
+ *     path) or FP32 (val_bits 32, the twin that the unchanged <int32_t,float>
+ *     Trident drivers link against).
+ *   - Every call is stream-ordered on the caller's stream (a cudaStream_t
+ *     passed as void*; NULL is the legacy default stream).  Calls that must
+ *     return a size to the host synchronise that stream and say so.
+ *   - A context owns its workspace pool; it is not thread-safe.  Use one
+ *     context per host thread (Trident's main and accumulation threads each
+ *     get their own).  There is no global mutable state.
+ *   - Functions return a TSPG_* status; nothing in the library exits.
+ *   - Output rows of SpGEMM, SpGEMM-accumulate and spadd are sorted by column
+ *     with no duplicate columns.  Structural zeros are kept (an entry whose
+ *     value cancels to 0.0 stays in the pattern), matching KokkosKernels and
+ *     csrgeam2 as Trident uses them.  spadd and the C_in operand of
+ *     tspg_spgemm_acc require sorted, duplicate-free rows.
+ */
+#ifndef TSPG_H
+#define TSPG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSPG_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+  TSPG_OK = 0,
+  TSPG_EINVAL = 1,     /* bad argument (null pointer, bad bits, shape mismatch) */
+  TSPG_ENOMEM = 2,     /* workspace beyond the context budget, or an output
+                          buffer too small and no allocator given (the needed
+                          size is still reported) */
+  TSPG_EOVERFLOW = 3,  /* int32 row offsets requested but nnz > INT32_MAX */
+  TSPG_ETIMEOUT = 4,   /* a bounded device wait gave up */
+  TSPG_ECUDA = 5,      /* a CUDA runtime call failed (see tspg_last_cuda_error) */
+  TSPG_EUNSORTED = 6   /* an operand that must have sorted rows does not */
+};
+
+/* Major dimension of a compressed sparse matrix (mmio::MajorDim). */
+enum { TSPG_ROWS = 0, TSPG_COLS = 1 };
+
+/* Flags for the SpGEMM entry points. */
+enum {
+  TSPG_F_NONE = 0,
+  /* Skip the device check that B's rows are sorted; the caller promises they
+     are.  Without it the library checks and, for unsorted B, uses the
+     cursor-free form of the long-row kernel. */
+  TSPG_F_B_SORTED = 1
+};
+
+/* Read-only sparse operand (CSR; for the pack, the compressed dimension is
+   given separately). */
+typedef struct tspg_csr {
+  int64_t nrows;
+  int64_t ncols;
+  int64_t nnz;
+  const void *rowptr;  /* (major dim + 1) offsets, int32 or int64 */
+  int32_t rowptr_bits; /* 32 | 64 */
+  int32_t val_bits;    /* 32 | 64 */
+  const int32_t *col;  /* nnz column (or row, for CSC) indices */
+  const void *val;     /* nnz values */
+} tspg_csr;
+
+/* Device allocator callback: returns a device pointer of at least `bytes`
+   bytes usable on `stream`, or NULL.  The library never frees it. */
+typedef void *(*tspg_alloc_fn)(void *user, size_t bytes, void *stream);
+
+/* Sparse result.  The caller provides rowptr (nrows+1 entries of
+   rowptr_bits).  col/val either point to `capacity` entries each, or are
+   allocated through `alloc` when capacity < nnz (mirrors
+   CsxBuffers::ensure_async in include/utils.cuh:685-728).  On return nnz holds
+   the result size, also when the call fails with TSPG_ENOMEM because the
+   capacity was short and alloc is NULL. */
+typedef struct tspg_csr_out {
+  int64_t nrows;
+  int64_t ncols;
+  int64_t nnz;      /* out */
+  void *rowptr;
+  int32_t rowptr_bits;
+  int32_t val_bits;
+  int32_t *col;
+  void *val;
+  int64_t capacity; /* entries available in col and val */
+  tspg_alloc_fn alloc;
+  void *alloc_user;
+} tspg_csr_out;
+
+typedef struct tspg_ctx tspg_ctx;
+typedef struct tspg_plan tspg_plan;
+
+/* ---- library and context -------------------------------------------------
+ * Replaces: the cusparseHandle_t + CsxBuffers temp buffers + setup_mempool
+ * (include/mempool.cuh:9-22) that every Trident rank holds.  The context owns
+ * a cudaMemPool with release threshold UINT64_MAX, so workspace stays
+ * resident between calls; `pool_budget` bytes (0 = no limit) caps what the
+ * library itself may hold. */
+int tspg_abi_version(void);
+const char *tspg_strerror(int status);
+int tspg_last_cuda_error(const tspg_ctx *ctx);
+int tspg_ctx_create(int device, size_t pool_budget, tspg_ctx **out);
+int tspg_ctx_destroy(tspg_ctx *ctx);
+/* Bytes of workspace the context holds now / at most so far. */
+int tspg_ctx_mem(const tspg_ctx *ctx, size_t *in_use, size_t *high_water);
+/* Instrumentation.  tspg_ctx_stats: library kernels launched through this
+ * context so far (kernels inside replayed CUDA graphs included).
+ * tspg_ctx_phase_timing: when enabled, every SpGEMM call records CUDA events
+ * on its stream around its persistent symbolic and numeric kernels;
+ * tspg_ctx_phase_ms waits for and returns those two durations of the last
+ * call (the NVTX / CUDA_TIMER_* role of the reference, src/hns_spgemm.cu
+ * :755-1042). */
+int tspg_ctx_stats(const tspg_ctx *ctx, int64_t *launches);
+int tspg_ctx_phase_timing(tspg_ctx *ctx, int enable);
+int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
+
+/* ---- SpGEMM ----------------------------------------------------------------
+ * tspg_spgemm_count — the flop-count pass.  mults = sum over A's nonzeros
+ * (i,k) of nnz(B row k) (cusparseSpGEMM_getNumProducts,
+ * include/cusparse_helpers.cuh:981-985,1251-1257); c_nnz_upper =
+ * sum_i min(mults_i, ncols(B)), the admission bound on nnz(C).  Synchronises
+ * `stream`. */
+int tspg_spgemm_count(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                      const tspg_csr *B, int64_t *mults, int64_t *c_nnz_upper);
+
+/* tspg_spgemm — C = A·B, two-phase inside (symbolic, then numeric).
+ * Replaces LocalMatrix::spgemm (include/KokkosWrap.hpp:367-391) and
+ * cusparse_spgemm / _reuse / _mem (include/cusparse_helpers.cuh:908-1344).
+ * Empty operands give an empty C with a zeroed rowptr (the num_prods == 0
+ * exit, include/cusparse_helpers.cuh:1251-1257).  Synchronises `stream` once
+ * (to learn nnz(C)). */
+int tspg_spgemm(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                const tspg_csr *B, tspg_csr_out *C, int flags);
+
+/* Split form for structure reuse (cusparse_spgemm_reuse,
+ * include/cusparse_helpers.cuh:1023-1189): the symbolic phase returns nnz(C)
+ * and keeps the row structure in `plan`; numeric may then run any number of
+ * times for operands with the same pattern and new values.  The plan borrows
+ * nothing; destroy it with tspg_plan_destroy. */
+int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                         const tspg_csr *B, int flags, tspg_plan **plan,
+                         int64_t *c_nnz);
+int tspg_spgemm_numeric(tspg_ctx *ctx, void *stream, tspg_plan *plan,
+                        const tspg_csr *A, const tspg_csr *B,
+                        tspg_csr_out *C);
+int tspg_plan_destroy(tspg_plan *plan);
+
+/* tspg_spgemm_acc — C_out = C_in + A·B with the union pattern.  Replaces
+ * LocalMatrix::sp_mma (include/KokkosWrap.hpp:315-364), sp_mma_hybrid
+ * (include/cusparse_helpers.cuh:708-739) and cusparse_spmma
+ * (include/cusparse_helpers.cuh:744-796).  C_in may be NULL or empty (the
+ * "first product" case, KokkosWrap.hpp:334-338); then C_out = A·B. */
+int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                    const tspg_csr *B, const tspg_csr *C_in,
+                    tspg_csr_out *C_out, int flags);
+
+/* ---- merge ------------------------------------------------------------------
+ * tspg_spadd — C = A + B, union pattern, alpha = beta = 1.  Replaces
+ * cusparse_spgeam (include/cusparse_helpers.cuh:799-905) and
+ * LocalMatrix::spadd (include/KokkosWrap.hpp:394-439).  Rows of A and B must
+ * be sorted and duplicate-free.  Synchronises `stream` once. */
+int tspg_spadd(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+               const tspg_csr *B, tspg_csr_out *C);
+
+/* ---- bitmask tile pack --------------------------------------------------------
+ * tspg_bitmask_gen — mask byte w bit b (LSB first) is set iff segment 8w+b of
+ * `ptr` is non-empty (ptr[i] != ptr[i+1]); n segments, ceil(n/8) bytes out.
+ * Replaces SpaComm::gen_bitmask (include/spacomm.cuh:29-117) with
+ * MASK_SIZE = 8, BMASK_TYPE = uint8_t (include/common.h:63-65). */
+int tspg_bitmask_gen(tspg_ctx *ctx, void *stream, const void *ptr,
+                     int ptr_bits, int64_t n, uint8_t *mask_out);
+
+/* tspg_bitmask_and — out = a & b bytewise (SpaComm::intersect_bitmasks,
+ * include/spacomm.cuh:126-148).  `out` may alias a or b. */
+int tspg_bitmask_and(tspg_ctx *ctx, void *stream, const uint8_t *a,
+                     const uint8_t *b, int64_t nbytes, uint8_t *out);
+
+/* tspg_pack — SpaCommHandler::Compress (include/spacomm.cuh:962-1091) on one
+ * tile: keep the entries of every segment (row for TSPG_ROWS, column for
+ * TSPG_COLS) whose mask bit is set, in their original order; the pointer
+ * array keeps its full length with masked segments made empty
+ * (select_ptrs, include/spacomm.cuh:556-623).  Output wire layout in
+ * `out_buf` (TileHolder::set_csx_ptrs, include/tile_holder.cuh:80-89):
+ *     [ val[nnz_kept] | idx int32[nnz_kept] | ptr[len+1] ]
+ * with val of M->val_bits and ptr of M->rowptr_bits.  `cap` must be at least
+ * the unpacked tile's size, nnz*(val+4) + (len+1)*ptr bytes.  When
+ * `nnz_kept_host` is non-NULL the call synchronises `stream` and stores the
+ * kept count there; it is always also written to `nnz_kept_dev` when that is
+ * non-NULL (device int64). */
+int tspg_pack(tspg_ctx *ctx, void *stream, const tspg_csr *M, int major,
+              const uint8_t *mask, void *out_buf, size_t cap,
+              int64_t *nnz_kept_dev, int64_t *nnz_kept_host);
+
+/* Size in bytes of a packed tile (CSX_buf_size / compute_message_size,
+ * src/hns_spgemm.cu:23-26). */
+size_t tspg_packed_bytes(int64_t nnz, int64_t ptr_len, int val_bits,
+                         int ptr_bits);
+
+/* tspg_unpack — the receiver side: wrap a packed buffer as a CSX view
+ * (TileHolder::form_mmiocsx, include/tile_holder.cuh:212-233).  Host-only
+ * pointer arithmetic; the view borrows `buf`. */
+int tspg_unpack(const void *buf, int64_t nrows, int64_t ncols, int major,
+                int64_t nnz, int val_bits, int ptr_bits, tspg_csr *out);
+
+/* ---- batched products ----------------------------------------------------------
+ * Many independent products C_i = A_i·B_i of uneven sizes in one persistent
+ * launch per phase, fed by a device work queue; each phase is a CUDA graph
+ * captured on the first run and replayed while the batch is unchanged.
+ * Outputs go to one slab owned by the batch (context pool, reused across
+ * runs); read each result with tspg_batch_result, valid until the next run,
+ * clear or destroy.  All products of a batch share the rowptr and value
+ * widths.  The batch borrows its operands: they must stay valid and
+ * unchanged in shape while it is used. */
+typedef struct tspg_batch tspg_batch;
+int tspg_batch_create(tspg_ctx *ctx, tspg_batch **out);
+int tspg_batch_destroy(tspg_batch *b);
+int tspg_batch_clear(tspg_batch *b);
+int tspg_batch_add(tspg_batch *b, const tspg_csr *A, const tspg_csr *B,
+                   int *index_out);
+/* Runs all products; synchronises `stream` once (for the output size). */
+int tspg_batch_run(tspg_batch *b, void *stream, int flags,
+                   int64_t *total_nnz);
+/* View of result i (device pointers into the batch's slab, int64 rowptr). */
+int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out);
+
+/* ---- synthetic inputs (host) -----------------------------------------------------
+ * Seeded generators of the benchmark operands, host memory, int64 rowptr.
+ * Arrays are allocated with malloc and released with tspg_host_free. */
+typedef struct tspg_host_csr {
+  int64_t nrows, ncols, nnz;
+  int64_t *rowptr;
+  int32_t *col;
+  double *val;
+} tspg_host_csr;
+void tspg_host_free(tspg_host_csr *M);
+/* n x n, row i = k distinct uniform columns plus (if diag) column i. */
+int tspg_gen_uniform_rows(int64_t n, int k, int diag, uint64_t seed,
+                          tspg_host_csr *out);
+/* R-MAT: 2^scale rows, edge_factor*2^scale draws, quadrant probabilities
+ * a, b, c (d = 1-a-b-c), duplicates merged, self-loops kept. */
+int tspg_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                  uint64_t seed, tspg_host_csr *out);
+/* 27-point (pts=27, 26 / -1) or 7-point (pts=7, 6 / -1) Laplacian on an
+ * nx*ny*nz grid, lexicographic x-fastest numbering. */
+int tspg_gen_laplacian(int64_t nx, int64_t ny, int64_t nz, int pts,
+                       tspg_host_csr *out);
+/* Smoothed-aggregation prolongator P = (I - omega D^-1 A) P_tent for a
+ * Laplacian A from tspg_gen_laplacian, aggregates agg^3 by integer division
+ * of the grid coordinates, P_tent 0/1 (unnormalised). */
+int tspg_gen_sa_prolongator(int64_t nx, int64_t ny, int64_t nz, int pts,
+                            int agg, double omega, tspg_host_csr *out);
+/* Host transpose (R = P^T for the Galerkin product). */
+int tspg_host_transpose(const tspg_host_csr *M, tspg_host_csr *out);
+/* Random square matrix of the batched workload: rows x rows, row lengths
+ * Poisson(lambda), distinct uniform columns. */
+int tspg_gen_poisson_rows(int64_t rows, double lambda, uint64_t seed,
+                          tspg_host_csr *out);
+/* Read a Trident .bmtx file (MatrixMarket banner with index and value byte
+ * widths, then little-endian (row, col, float32) records) into CSR with
+ * duplicates kept in file order. */
+int tspg_read_bmtx(const char *path, tspg_host_csr *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSPG_H */

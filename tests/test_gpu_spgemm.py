@@ -1,0 +1,165 @@
+"""GPU parity: SpGEMM through the C ABI against the oracle on the same inputs.
+
+Structure (rowptr, sorted columns) must be bit-exact; FP64 values within
+|x - y| <= 1e-12 * max(|y|, sum |a_ik b_kj|) per entry (summation order only).
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from helpers import TOL32, check_product, random_csr
+from trident_b200 import ops, workloads
+from trident_b200._lib import TSPG_EINVAL, TSPG_F_B_SORTED, TspgError
+from trident_b200.csr import HostCSR
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("rp_in,rp_out", [(32, 64), (64, 32), (32, 32), (64, 64)])
+def test_uniform_rows_1024(ctx, rp_in, rp_out):
+    A = workloads.uniform_rows(1024, 16, True, seed=1)
+    dA = A.to_device(rowptr_bits=rp_in)
+    C = ops.spgemm(ctx, dA, dA, rowptr_bits=rp_out)
+    assert C.rowptr.dtype == (torch.int32 if rp_out == 32 else torch.int64)
+    check_product(C, A, A)
+
+
+@pytest.mark.parametrize("name", ["n16_full.bmtx", "n1024.bmtx"])
+def test_bmtx_fixtures(ctx, name):
+    A = workloads.read_bmtx(os.path.join(GOLD, name))
+    dA = A.to_device()
+    check_product(ops.spgemm(ctx, dA, dA), A, A)
+
+
+@pytest.mark.parametrize("scale", [8, 11, 13])
+def test_rmat(ctx, scale):
+    A = workloads.rmat(scale=scale, edge_factor=16, seed=1)
+    dA = A.to_device()
+    check_product(ops.spgemm(ctx, dA, dA), A, A)
+
+
+def test_rmat_scale15_all_classes(ctx):
+    # scale 15 R-MAT squared has rows in every class, DENSE symbolic included
+    A = workloads.rmat(scale=15, edge_factor=16, seed=2)
+    dA = A.to_device()
+    mults = oracle.row_mults(A, A)
+    assert mults.max() > 24576
+    check_product(ops.spgemm(ctx, dA, dA), A, A)
+
+
+def test_dense_numeric_rows_multiwindow(ctx):
+    # a few rows whose products hit > 8192 distinct columns over 3 windows of
+    # 16384 columns: the DENSE numeric class with cursors
+    rng = np.random.default_rng(4)
+    n = 40000
+    B = random_csr(3000, n, per_row=40, seed=5)
+    A = random_csr(64, 3000, per_row=4, seed=6)
+    heavy = random_csr(3, 3000, per_row=800, seed=7)
+    Ah = HostCSR(67, 3000, np.concatenate([A.rowptr, A.rowptr[-1] + heavy.rowptr[1:]]),
+                 np.concatenate([A.col, heavy.col]), np.concatenate([A.val, heavy.val]))
+    C = ops.spgemm(ctx, Ah.to_device(), B.to_device())
+    H = check_product(C, Ah, B)
+    assert np.diff(H.rowptr).max() > 8192
+
+
+def test_dense_numeric_long_a_row_global_cursors(ctx):
+    # one A row with > 8192 entries: cursors live in the global scratch
+    B = random_csr(20000, 30000, per_row=3, seed=8)
+    A = random_csr(2, 20000, per_row=9000, seed=9)
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+
+
+def test_unsorted_and_duplicate_b_rows(ctx):
+    B = random_csr(500, 20000, per_row=60, seed=10, sort=False)
+    A = random_csr(300, 500, per_row=200, seed=11)  # several DENSE numeric rows
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+    Bd = random_csr(400, 300, per_row=30, seed=12, sort=False, dup=True)
+    Ad = random_csr(200, 400, per_row=10, seed=13, dup=True)
+    check_product(ops.spgemm(ctx, Ad.to_device(), Bd.to_device()), Ad, Bd)
+
+
+def test_galerkin_rap_small(ctx):
+    R, A, P = workloads.galerkin_operands(n=18, pts=27, agg=3)
+    dR, dA, dP = R.to_device(), A.to_device(), P.to_device()
+    AP = ops.spgemm(ctx, dA, dP, rowptr_bits=32)
+    hAP = check_product(AP, A, P)
+    RAP = ops.spgemm(ctx, dR, AP)
+    check_product(RAP, R, hAP)
+
+
+def test_poisson_rows(ctx):
+    A = workloads.poisson_rows(5000, 24.0, seed=3)
+    B = workloads.poisson_rows(5000, 24.0, seed=4)
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+
+
+def test_empty_cases(ctx):
+    E = HostCSR(0, 5, np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    B = random_csr(5, 7, density=0.5, seed=1)
+    C = ops.spgemm(ctx, E.to_device(), B.to_device())
+    assert C.nrows == 0 and C.nnz == 0 and C.rowptr.cpu().tolist() == [0]
+    Z = HostCSR(6, 5, np.zeros(7, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    C = ops.spgemm(ctx, Z.to_device(), B.to_device())
+    assert C.nnz == 0 and C.rowptr.cpu().tolist() == [0] * 7
+    A = random_csr(6, 5, density=0.5, seed=2)
+    BZ = HostCSR(5, 7, np.zeros(6, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    C = ops.spgemm(ctx, A.to_device(), BZ.to_device())
+    assert C.nnz == 0
+    # some empty rows mixed in
+    A2 = random_csr(100, 50, density=0.05, seed=3)
+    B2 = random_csr(50, 80, density=0.05, seed=4)
+    check_product(ops.spgemm(ctx, A2.to_device(), B2.to_device()), A2, B2)
+
+
+def test_structural_zero_kept(ctx):
+    A = HostCSR(1, 2, np.array([0, 2]), np.array([0, 1], np.int32), np.array([1.0, 1.0]))
+    B = HostCSR(2, 1, np.array([0, 1, 2]), np.array([0, 0], np.int32), np.array([1.0, -1.0]))
+    C = ops.spgemm(ctx, A.to_device(), B.to_device()).to_host()
+    assert C.rowptr.tolist() == [0, 1] and C.col.tolist() == [0] and C.val[0] == 0.0
+
+
+def test_fp32_twin(ctx):
+    A = workloads.rmat(scale=11, edge_factor=8, seed=3)
+    dA = A.to_device(val_bits=32)
+    A32 = HostCSR(A.nrows, A.ncols, A.rowptr, A.col, A.val.astype(np.float32).astype(np.float64))
+    check_product(ops.spgemm(ctx, dA, dA), A32, A32, tol=TOL32)
+
+
+def test_plan_reuse_new_values(ctx):
+    A = workloads.rmat(scale=10, edge_factor=16, seed=5)
+    dA = A.to_device()
+    plan = ops.Plan(ctx, dA, dA)
+    C1 = plan.numeric(dA, dA)
+    check_product(C1, A, A)
+    A2 = HostCSR(A.nrows, A.ncols, A.rowptr, A.col, -2.0 * A.val)
+    dA2 = A2.to_device()
+    C2 = plan.numeric(dA2, dA2)
+    check_product(C2, A2, A2)
+    plan.close()
+
+
+def test_count_pass(ctx):
+    A = workloads.rmat(scale=11, edge_factor=16, seed=6)
+    dA = A.to_device()
+    mults, upper = ops.spgemm_count(ctx, dA, dA)
+    rm = oracle.row_mults(A, A)
+    assert mults == int(rm.sum())
+    assert upper == int(np.minimum(rm, A.ncols).sum())
+
+
+def test_shape_mismatch_rejected(ctx):
+    A = random_csr(4, 5, density=0.5, seed=1).to_device()
+    B = random_csr(6, 7, density=0.5, seed=2).to_device()
+    with pytest.raises(TspgError) as e:
+        ops.spgemm(ctx, A, B)
+    assert e.value.status == TSPG_EINVAL
+
+
+def test_sorted_flag_skips_check(ctx):
+    A = workloads.uniform_rows(2048, 16, True, seed=7)
+    dA = A.to_device()
+    check_product(ops.spgemm(ctx, dA, dA, flags=TSPG_F_B_SORTED), A, A)

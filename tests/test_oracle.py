@@ -1,0 +1,139 @@
+"""CPU: the oracle against the reference's known answers and independent checks."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from helpers import random_csr
+from trident_b200 import workloads
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _kat():
+    with open(os.path.join(GOLD, "kat_bitmask.json")) as fh:
+        return json.load(fh)
+
+
+def test_gen_bitmask_kats():
+    for case in _kat()["gen_bitmask"]:
+        ptr = np.array(case["ptr"])
+        assert list(oracle.bitmask_gen(ptr, len(ptr) - 1)) == case["mask"]
+
+
+def test_intersect_kat():
+    for case in _kat()["intersect_bitmasks"]:
+        assert list(oracle.bitmask_and(case["a"], case["b"])) == case["out"]
+
+
+def test_tmp_test1_pack_kat():
+    k = _kat()["tmp_test1"]
+    ptr, idx, val = oracle.pack(np.array(k["ptr"]), np.array(k["col"]), np.array(k["val"]),
+                                np.array(k["mask"], dtype=np.uint8))
+    assert list(ptr) == k["expect_ptr"]
+    assert list(idx) == k["expect_col"]
+    assert list(val) == k["expect_val"]
+    assert len(idx) == k["expect_nnz"]
+
+
+def _dense(M):
+    D = np.zeros((M.nrows, M.ncols))
+    for i in range(M.nrows):
+        for p in range(M.rowptr[i], M.rowptr[i + 1]):
+            D[i, M.col[p]] += M.val[p]
+    return D
+
+
+def _pattern(M):
+    D = np.zeros((M.nrows, M.ncols), dtype=bool)
+    for i in range(M.nrows):
+        D[i, M.col[M.rowptr[i]:M.rowptr[i + 1]]] = True
+    return D
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_spgemm_vs_dense(seed):
+    A = random_csr(37, 29, density=0.15, seed=seed)
+    B = random_csr(29, 41, density=0.2, seed=seed + 100)
+    rp, cj, cx, ca = oracle.spgemm(A, B)
+    P = (_pattern(A).astype(int) @ _pattern(B).astype(int)) > 0
+    D = _dense(A) @ _dense(B)
+    for i in range(A.nrows):
+        cols = cj[rp[i]:rp[i + 1]]
+        assert list(cols) == sorted(np.nonzero(P[i])[0])
+        np.testing.assert_allclose(cx[rp[i]:rp[i + 1]], D[i, cols], rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(ca, np.abs(ca))
+
+
+def test_structural_zero_kept():
+    from trident_b200.csr import HostCSR
+    A = HostCSR(1, 2, np.array([0, 2]), np.array([0, 1], np.int32), np.array([1.0, 1.0]))
+    B = HostCSR(2, 1, np.array([0, 1, 2]), np.array([0, 0], np.int32), np.array([1.0, -1.0]))
+    rp, cj, cx, ca = oracle.spgemm(A, B)
+    assert list(rp) == [0, 1] and list(cj) == [0] and cx[0] == 0.0 and ca[0] == 2.0
+
+
+def test_spgemm_row_range_matches_full():
+    A = random_csr(60, 50, density=0.1, seed=5)
+    B = random_csr(50, 70, density=0.1, seed=6)
+    rp, cj, cx, _ = oracle.spgemm(A, B)
+    rp2, cj2, cx2, _ = oracle.spgemm(A, B, 17, 44)
+    np.testing.assert_array_equal(rp2, rp[17:45] - rp[17])
+    np.testing.assert_array_equal(cj2, cj[rp[17]:rp[44]])
+    np.testing.assert_array_equal(cx2, cx[rp[17]:rp[44]])
+
+
+def test_spadd_vs_dense():
+    A = random_csr(30, 40, density=0.2, seed=3)
+    B = random_csr(30, 40, density=0.2, seed=4)
+    cp, cj, cx = oracle.spadd(A, B)
+    P = _pattern(A) | _pattern(B)
+    D = _dense(A) + _dense(B)
+    for i in range(30):
+        cols = cj[cp[i]:cp[i + 1]]
+        assert list(cols) == list(np.nonzero(P[i])[0])
+        np.testing.assert_allclose(cx[cp[i]:cp[i + 1]], D[i, cols], rtol=1e-15, atol=0)
+
+
+def test_pack_keeps_masked_segments():
+    M = random_csr(50, 20, density=0.3, seed=9)
+    rng = np.random.default_rng(1)
+    mask = rng.integers(0, 256, size=(50 + 7) // 8, dtype=np.uint8)
+    ptr, idx, val = oracle.pack(M.rowptr, M.col, M.val, mask)
+    o = 0
+    for r in range(50):
+        seg = slice(M.rowptr[r], M.rowptr[r + 1])
+        keep = (mask[r // 8] >> (r % 8)) & 1
+        n = (M.rowptr[r + 1] - M.rowptr[r]) if keep else 0
+        assert ptr[r + 1] - ptr[r] == n
+        if keep:
+            np.testing.assert_array_equal(idx[o:o + n], M.col[seg])
+            np.testing.assert_array_equal(val[o:o + n], M.val[seg])
+        o += n
+
+
+def test_bmtx_fixture_digests():
+    import hashlib
+    with open(os.path.join(GOLD, "oracle_bmtx.json")) as fh:
+        gold = json.load(fh)
+    for name, g in gold.items():
+        A = workloads.read_bmtx(os.path.join(GOLD, name))
+        assert A.nrows == g["nrows"] and A.nnz == g["nnz_A"]
+        rp, cj, cx, ca = oracle.spgemm(A, A)
+        assert int(rp[-1]) == g["nnz_C"]
+        assert hashlib.sha256(np.ascontiguousarray(rp).tobytes()).hexdigest() == g["rowptr_sha256"]
+        assert hashlib.sha256(np.ascontiguousarray(cj).tobytes()).hexdigest() == g["col_sha256"]
+        assert abs(float(np.sum(cx)) - g["val_sum"]) <= 1e-9 * abs(g["val_sum"])
+
+
+def test_bmtx_values_vs_scipy():
+    A = workloads.read_bmtx(os.path.join(GOLD, "n1024.bmtx"))
+    rp, cj, cx, _ = oracle.spgemm(A, A)
+    S = (A.to_scipy() @ A.to_scipy()).tocsr()
+    S.sort_indices()
+    # fixture values are in [1, 2], so no cancellation: scipy keeps every entry
+    np.testing.assert_array_equal(S.indptr, rp)
+    np.testing.assert_array_equal(S.indices, cj)
+    np.testing.assert_allclose(S.data, cx, rtol=1e-13)

@@ -1,0 +1,186 @@
+// internal.cuh — shared internals of libtspg: the context, its stream-ordered
+// workspace pool, status plumbing and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <mutex>
+#include <unordered_map>
+
+#include "tspg.h"
+
+struct tspg_ctx {
+  int device = 0;
+  int num_sms = 0;
+  size_t smem_optin = 0;
+  cudaMemPool_t pool = nullptr;
+  size_t budget = 0;  // 0 = unlimited
+  size_t in_use = 0;
+  size_t high_water = 0;
+  int last_cuda = 0;
+  // pinned host words for small read-backs (sizes, flags)
+  int64_t *h_words = nullptr;
+  // device words: error flag and small counters that live with the context
+  int64_t *d_words = nullptr;
+  std::unordered_map<void *, size_t> live;
+  // instrumentation
+  int64_t launches = 0;        // library kernels launched (graph nodes included)
+  bool phase_timing = false;   // record events around the persistent phases
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool ev_sym = false, ev_num = false;
+};
+
+namespace tspg {
+
+constexpr int kHostWords = 64;
+constexpr int kDevWords = 64;
+// d_words slots
+constexpr int kErrWord = 0;  // device-side error code (0 = ok)
+
+#define TSPG_CUDA(ctx, ...)                                   \
+  do {                                                        \
+    cudaError_t _e = (__VA_ARGS__);                           \
+    if (_e != cudaSuccess) {                                  \
+      (ctx)->last_cuda = (int)_e;                             \
+      return TSPG_ECUDA;                                      \
+    }                                                         \
+  } while (0)
+
+#define TSPG_TRY(...)                 \
+  do {                                \
+    int _s = (__VA_ARGS__);           \
+    if (_s != TSPG_OK) return _s;     \
+  } while (0)
+
+// Event pair k (0: symbolic phase, 1: numeric phase) around a k_phase launch.
+inline void phase_mark(tspg_ctx *ctx, int k, int edge, cudaStream_t s) {
+  if (!ctx->phase_timing) return;
+  cudaEventRecord(ctx->ev[2 * k + edge], s);
+  if (edge == 1) (k == 0 ? ctx->ev_sym : ctx->ev_num) = true;
+}
+
+// Stream-ordered workspace from the context pool, with the budget enforced.
+int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
+void ws_free(tspg_ctx *ctx, void *p, cudaStream_t s);
+
+// RAII list of workspace blocks released at scope exit on one stream.
+struct Scratch {
+  tspg_ctx *ctx;
+  cudaStream_t s;
+  void *ptrs[32];
+  int n = 0;
+  Scratch(tspg_ctx *c, cudaStream_t st) : ctx(c), s(st) {}
+  template <typename T>
+  int get(T **p, size_t count) {
+    void *q = nullptr;
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    int st = ws_alloc(ctx, &q, bytes, s);
+    if (st != TSPG_OK) return st;
+    ptrs[n++] = q;
+    *p = (T *)q;
+    return TSPG_OK;
+  }
+  ~Scratch() {
+    for (int i = n - 1; i >= 0; --i) ws_free(ctx, ptrs[i], s);
+  }
+};
+
+inline int check_csr(const tspg_csr *M) {
+  if (!M) return TSPG_EINVAL;
+  if (M->nrows < 0 || M->ncols < 0 || M->nnz < 0) return TSPG_EINVAL;
+  if (M->rowptr_bits != 32 && M->rowptr_bits != 64) return TSPG_EINVAL;
+  if (M->val_bits != 32 && M->val_bits != 64) return TSPG_EINVAL;
+  if (M->ncols > INT32_MAX) return TSPG_EINVAL;  // int32 column indices
+  if (M->rowptr_bits == 32 && M->nnz > INT32_MAX) return TSPG_EOVERFLOW;
+  if (M->nnz > 0 && (!M->col || !M->val)) return TSPG_EINVAL;
+  if (!M->rowptr && M->nrows > 0) return TSPG_EINVAL;
+  return TSPG_OK;
+}
+
+// ---------------------------------------------------------------- device side
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// Inclusive warp scan.
+template <typename T>
+__device__ __forceinline__ T warp_scan_incl(T v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T w = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += w;
+  }
+  return v;
+}
+
+// Synchronise a group of G threads (G = 32, 1024, or a named-barrier group).
+template <int G>
+__device__ __forceinline__ void group_sync(int gid) {
+  if constexpr (G == 32) {
+    __syncwarp();
+  } else if constexpr (G >= 1024) {
+    __syncthreads();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(G) : "memory");
+  }
+}
+
+// Exclusive scan across a group of G threads; `tmp` holds G/32 + 1 ints of
+// shared memory private to the group.  Returns the exclusive prefix; the group
+// total goes to *total.
+template <int G, typename T>
+__device__ __forceinline__ T group_excl_scan(T v, T *tmp, int gid, T *total) {
+  const int lane = threadIdx.x & 31;
+  T inc = warp_scan_incl(v);
+  if constexpr (G == 32) {
+    *total = __shfl_sync(0xffffffffu, inc, 31);
+    return inc - v;
+  } else {
+    constexpr int NW = G / 32;
+    const int w = (threadIdx.x % G) >> 5;
+    if (lane == 31) tmp[w] = inc;
+    group_sync<G>(gid);
+    if (w == 0) {
+      T x = lane < NW ? tmp[lane] : T(0);
+      T xi = warp_scan_incl(x);
+      if (lane < NW) tmp[lane] = xi - x;
+      if (lane == NW - 1) tmp[NW] = xi;
+    }
+    group_sync<G>(gid);
+    T res = tmp[w] + inc - v;
+    *total = tmp[NW];
+    group_sync<G>(gid);
+    return res;
+  }
+}
+
+template <int G, typename T>
+__device__ __forceinline__ T group_sum(T v, T *tmp, int gid) {
+  T total;
+  group_excl_scan<G, T>(v, tmp, gid, &total);
+  return total;
+}
+
+__device__ __forceinline__ void set_error(int64_t *err, int code) {
+  atomicCAS((unsigned long long *)err, 0ull, (unsigned long long)code);
+}
+
+}  // namespace tspg

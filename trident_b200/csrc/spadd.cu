@@ -1,0 +1,167 @@
+// spadd.cu — merge of partial C tiles, C = A + B with the union pattern.
+//
+// Replaces cusparse_spgeam (include/cusparse_helpers.cuh:799-905: csrgeam2
+// bufferSize + Nnz + compute, five stream syncs, the nnz through the host) and
+// LocalMatrix::spadd (include/KokkosWrap.hpp:394-439: KK spadd symbolic +
+// numeric).  Rows are sorted and duplicate-free, so every entry finds its
+// output slot independently: an A entry at row position i lands at
+// i + |{b in B row : b < a}|, a B entry that is not in A at
+// j + |{a in A row : a < b}|.  One warp per row; lanes take entries and binary
+// search the other row (which sits in L1 after the first probes).
+#include "internal.cuh"
+#include "spgemm_kernels.cuh"
+
+namespace tspg {
+
+template <typename IT>
+__device__ __forceinline__ int64_t lower_bound_row(const int32_t *col, int64_t lo,
+                                                   int64_t hi, int32_t x) {
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (__ldg(col + mid) < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+template <typename PTA, typename PTB>
+__global__ void __launch_bounds__(256)
+    k_spadd_count(int64_t m, const PTA *Ap, const int32_t *Aj, const PTB *Bp,
+                  const int32_t *Bj, int32_t *rowc) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = warp; r < m; r += nwarps) {
+    const int64_t a0 = Ap[r], a1 = Ap[r + 1], b0 = Bp[r], b1 = Bp[r + 1];
+    int dup = 0;
+    if (b1 > b0) {
+      for (int64_t p = a0 + lane; p < a1; p += 32) {
+        const int32_t x = __ldg(Aj + p);
+        const int64_t q = lower_bound_row<int>(Bj, b0, b1, x);
+        dup += (q < b1 && __ldg(Bj + q) == x);
+      }
+    }
+    dup = warp_sum(dup);
+    if (lane == 0) rowc[r] = int32_t((a1 - a0) + (b1 - b0) - dup);
+  }
+}
+
+template <typename PTA, typename PTB, typename VT>
+__global__ void __launch_bounds__(256)
+    k_spadd_fill(int64_t m, const PTA *Ap, const int32_t *Aj, const VT *Ax,
+                 const PTB *Bp, const int32_t *Bj, const VT *Bx,
+                 const int64_t *cp, void *Cp, int cp_bits, int32_t *Cj, VT *Cx) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = warp; r < m; r += nwarps) {
+    const int64_t a0 = Ap[r], a1 = Ap[r + 1], b0 = Bp[r], b1 = Bp[r + 1];
+    const int64_t o = cp[r];
+    if (lane == 0) {
+      if (cp_bits == 32) ((int32_t *)Cp)[r] = int32_t(o);
+      else ((int64_t *)Cp)[r] = o;
+      if (r == m - 1) {
+        if (cp_bits == 32) ((int32_t *)Cp)[m] = int32_t(cp[m]);
+        else ((int64_t *)Cp)[m] = cp[m];
+      }
+    }
+    for (int64_t p = a0 + lane; p < a1; p += 32) {
+      const int32_t x = __ldg(Aj + p);
+      const int64_t q = lower_bound_row<int>(Bj, b0, b1, x);
+      VT v = __ldg(Ax + p);
+      if (q < b1 && __ldg(Bj + q) == x) v += __ldg(Bx + q);
+      const int64_t pos = o + (p - a0) + (q - b0);
+      Cj[pos] = x;
+      Cx[pos] = v;
+    }
+    for (int64_t q = b0 + lane; q < b1; q += 32) {
+      const int32_t x = __ldg(Bj + q);
+      const int64_t p = lower_bound_row<int>(Aj, a0, a1, x);
+      if (p < a1 && __ldg(Aj + p) == x) continue;
+      const int64_t pos = o + (q - b0) + (p - a0);
+      Cj[pos] = x;
+      Cx[pos] = __ldg(Bx + q);
+    }
+  }
+}
+
+template <typename PTA, typename PTB, typename VT>
+static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
+                      const tspg_csr *B, tspg_csr_out *C) {
+  const int64_t m = A->nrows;
+  Scratch sc(ctx, s);
+  int32_t *rowc;
+  int64_t *cp, *partial;
+  const int64_t nb = (m + kScanTile - 1) / kScanTile;
+  Sched *dummy;
+  TSPG_TRY(sc.get(&rowc, m));
+  TSPG_TRY(sc.get(&cp, m + 1));
+  TSPG_TRY(sc.get(&partial, nb + 1));
+  TSPG_TRY(sc.get(&dummy, 1));
+  TSPG_CUDA(ctx, cudaMemsetAsync(cp, 0, sizeof(int64_t), s));
+  TSPG_CUDA(ctx, cudaMemsetAsync(dummy, 0, sizeof(Sched), s));
+  const unsigned grid = (unsigned)std::min<int64_t>((m * 32 + 255) / 256, int64_t(ctx->num_sms) * 16);
+  if (m > 0) {
+    k_spadd_count<PTA, PTB><<<grid, 256, 0, s>>>(m, (const PTA *)A->rowptr, A->col,
+                                                 (const PTB *)B->rowptr, B->col, rowc);
+    k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial);
+    k_scan_partials<<<1, 1024, 0, s>>>(partial, nb);
+    k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial, nb, cp, dummy);
+    ctx->launches += 4;
+  }
+  TSPG_CUDA(ctx, cudaGetLastError());
+  int64_t *h = ctx->h_words;
+  TSPG_CUDA(ctx, cudaMemcpyAsync(h, cp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  TSPG_CUDA(ctx, cudaStreamSynchronize(s));
+  const int64_t nnz = h[0];
+  if (C->rowptr_bits == 32 && nnz > INT32_MAX) return TSPG_EOVERFLOW;
+  C->nnz = nnz;
+  if (C->capacity < nnz) {
+    if (!C->alloc) return TSPG_ENOMEM;
+    void *cj = C->alloc(C->alloc_user, size_t(nnz) * 4, s);
+    void *cx = C->alloc(C->alloc_user, size_t(nnz) * sizeof(VT), s);
+    if (!cj || !cx) return TSPG_ENOMEM;
+    C->col = (int32_t *)cj;
+    C->val = cx;
+    C->capacity = nnz;
+  }
+  if (m == 0) {
+    TSPG_CUDA(ctx, cudaMemsetAsync(C->rowptr, 0, C->rowptr_bits / 8, s));
+    return TSPG_OK;
+  }
+  k_spadd_fill<PTA, PTB, VT><<<grid, 256, 0, s>>>(
+      m, (const PTA *)A->rowptr, A->col, (const VT *)A->val, (const PTB *)B->rowptr,
+      B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val);
+  ctx->launches += 1;
+  TSPG_CUDA(ctx, cudaGetLastError());
+  return TSPG_OK;
+}
+
+}  // namespace tspg
+
+using namespace tspg;
+
+extern "C" int tspg_spadd(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                          const tspg_csr *B, tspg_csr_out *C) {
+  if (!ctx || !C) return TSPG_EINVAL;
+  TSPG_TRY(check_csr(A));
+  TSPG_TRY(check_csr(B));
+  if (A->nrows != B->nrows || A->ncols != B->ncols || A->val_bits != B->val_bits)
+    return TSPG_EINVAL;
+  if (!C->rowptr || C->nrows != A->nrows || C->ncols != A->ncols ||
+      C->val_bits != A->val_bits || (C->rowptr_bits != 32 && C->rowptr_bits != 64))
+    return TSPG_EINVAL;
+  cudaStream_t s = (cudaStream_t)stream;
+  TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int a = A->rowptr_bits, b = B->rowptr_bits;
+  if (A->val_bits == 64) {
+    if (a == 32 && b == 32) return spadd_impl<int32_t, int32_t, double>(ctx, s, A, B, C);
+    if (a == 32 && b == 64) return spadd_impl<int32_t, int64_t, double>(ctx, s, A, B, C);
+    if (a == 64 && b == 32) return spadd_impl<int64_t, int32_t, double>(ctx, s, A, B, C);
+    return spadd_impl<int64_t, int64_t, double>(ctx, s, A, B, C);
+  } else {
+    if (a == 32 && b == 32) return spadd_impl<int32_t, int32_t, float>(ctx, s, A, B, C);
+    if (a == 32 && b == 64) return spadd_impl<int32_t, int64_t, float>(ctx, s, A, B, C);
+    if (a == 64 && b == 32) return spadd_impl<int64_t, int32_t, float>(ctx, s, A, B, C);
+    return spadd_impl<int64_t, int64_t, float>(ctx, s, A, B, C);
+  }
+}

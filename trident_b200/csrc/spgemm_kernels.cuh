@@ -1,0 +1,400 @@
+// spgemm_kernels.cuh — device side of the two-phase row-wise SpGEMM.
+//
+// Layout in HBM.  Operands are plain CSR (row offsets int32 or int64, int32
+// column indices, FP64 or FP32 values).  A launch covers one or many products
+// ("prods"); rows of all products are numbered globally (row g of product p
+// is g = base[p] + r) so that binning, scans and the persistent work queue
+// see one flat row space.  Per global row the plan keeps:
+//   rowf[g]  int64  products (a.k.a. mults / flops/2) of the row
+//   rowc[g]  int32  distinct output columns (symbolic result)
+//   cp[g]    int64  exclusive prefix of rowc over the flat row space
+//   list[]   uint64 rows binned by class, entry = (p << 40) | r
+//
+// Row classes (the same five for both phases, heaviest first so that the
+// persistent grid starts on the long rows):
+//   DENSE  one 1024-thread CTA per row, dense shared-memory window:
+//          symbolic = bitmap of up to 1.5M columns, numeric = FP64 window of
+//          16384 columns swept left to right with per-A-entry cursors into
+//          the sorted B rows; output is sorted by construction.
+//   G1024  one CTA per row, open-addressing hash in shared memory.
+//   G256   4 rows per CTA (256-thread groups, named barriers).
+//   G128   8 rows per CTA.
+//   G32    one warp per row, 2 rows per warp per work item.
+// Hash rows are sorted after accumulation by an in-place compaction into the
+// first half of the table and a bitonic sort of the compacted pairs.
+#pragma once
+
+#include "internal.cuh"
+
+namespace tspg {
+
+constexpr int kThreads = 1024;
+constexpr int kDynSmem = 196608;  // 192 KiB per CTA, one CTA per SM
+constexpr int NCLS = 5;
+enum { CLS_DENSE = 0, CLS_G1024 = 1, CLS_G256 = 2, CLS_G128 = 3, CLS_G32 = 4 };
+__host__ __device__ constexpr int cls_group(int c) {
+  return c <= CLS_G1024 ? 1024 : c == CLS_G256 ? 256 : c == CLS_G128 ? 128 : 32;
+}
+// rows handled by one work item of each class
+__host__ __device__ constexpr int cls_rows_per_item(int c) {
+  return c <= CLS_G1024 ? 1 : c == CLS_G256 ? 4 : c == CLS_G128 ? 8 : 64;
+}
+
+// Class limits (symbolic: on min(mults, ncols); numeric: on the row's nnz).
+// Symbolic tables hold int32 keys (128 KiB per CTA), numeric tables hold
+// key + FP64 value (192 KiB per CTA); a table has T = pow2 >= 2x the bound.
+__host__ __device__ constexpr int64_t kSymLim32 = 512, kSymLim128 = 2048,
+                                      kSymLim256 = 4096, kSymLim1024 = 24576;
+__host__ __device__ constexpr int64_t kNumLim32 = 256, kNumLim128 = 1024,
+                                      kNumLim256 = 2048, kNumLim1024 = 8192;
+constexpr int kSymT32 = 1024, kSymT128 = 4096, kSymT256 = 8192,
+              kSymT1024 = 32768;
+constexpr int kNumT32 = 512, kNumT128 = 2048, kNumT256 = 4096,
+              kNumT1024 = 16384;
+constexpr int kDenseW = 16384;           // numeric dense window (columns)
+constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory
+constexpr int64_t kDenseBits = int64_t(kDynSmem) * 8;  // symbolic bitmap
+
+__host__ __device__ inline int sym_class(int64_t f, int64_t n) {
+  const int64_t fe = f < n ? f : n;
+  if (f == 0) return -1;
+  if (fe <= kSymLim32) return CLS_G32;
+  if (fe <= kSymLim128) return CLS_G128;
+  if (fe <= kSymLim256) return CLS_G256;
+  if (fe <= kSymLim1024) return CLS_G1024;
+  return CLS_DENSE;
+}
+__host__ __device__ inline int num_class(int64_t c) {
+  if (c == 0) return -1;
+  if (c <= kNumLim32) return CLS_G32;
+  if (c <= kNumLim128) return CLS_G128;
+  if (c <= kNumLim256) return CLS_G256;
+  if (c <= kNumLim1024) return CLS_G1024;
+  return CLS_DENSE;
+}
+
+template <typename PT, typename VT>
+struct ProdDev {
+  const PT *Ap;
+  const int32_t *Aj;
+  const VT *Ax;
+  const PT *Bp;
+  const int32_t *Bj;
+  const VT *Bx;
+  int64_t m, n;
+  int32_t *Cj;
+  VT *Cx;
+  void *Cp;       // output rowptr (product-local), cp_bits wide
+  int32_t cp_bits;
+  int32_t b_sorted;
+};
+
+// Work schedule of one phase: rows per class, their list offsets and the
+// work-item prefix the persistent kernel decodes.
+struct Sched {
+  int64_t cnt[NCLS];
+  int64_t off[NCLS];
+  int64_t cur[NCLS];
+  int64_t items[NCLS + 1];
+  unsigned long long work;
+  int64_t total;      // sum of mults (symbolic) or of nnz (numeric)
+  int64_t upper;      // sum of min(mults, ncols)
+  int64_t max_a_row;  // longest A row (sizes the DENSE cursor scratch)
+  int64_t nonempty;
+  int64_t pad[3];
+};
+
+__device__ __forceinline__ int find_prod(const int64_t *base, int nprod,
+                                         int64_t g) {
+  int lo = 0, hi = nprod;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (base[mid] <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t col, int logT) {
+  return ((uint32_t)col * 2654435761u) >> (32 - logT);
+}
+
+__device__ __forceinline__ int ilog2_pow2(uint32_t x) { return 31 - __clz(x); }
+
+__device__ __forceinline__ uint32_t pow2_at_least(int64_t x, uint32_t lo) {
+  uint32_t t = lo;
+  while ((int64_t)t < x) t <<= 1;
+  return t;
+}
+
+// Threads of a sub-group walk one B row together; pick the sub-group width
+// from the average B-row length of this A row.
+__device__ __forceinline__ int subgroup_width(int64_t f, int64_t na, int G) {
+  int64_t avg = na > 0 ? f / na : 0;
+  int S = avg >= 24 ? 32 : avg >= 12 ? 16 : avg >= 6 ? 8 : avg >= 3 ? 4 : 2;
+  return S > G ? G : S;
+}
+
+// ---------------------------------------------------------------------------
+// Setup kernels
+
+template <typename PT, typename VT>
+__global__ void k_set_prod(ProdDev<PT, VT> *dst, ProdDev<PT, VT> v,
+                           int64_t *base, int64_t m) {
+  *dst = v;
+  base[0] = 0;
+  base[1] = m;
+}
+
+// New operand arrays for a plan's numeric re-run; the sortedness found by the
+// symbolic pass is kept.
+template <typename PT, typename VT>
+__global__ void k_set_operands(ProdDev<PT, VT> *dst, ProdDev<PT, VT> v) {
+  const int32_t sorted = dst->b_sorted;
+  *dst = v;
+  dst->b_sorted = sorted;
+}
+
+template <typename PT, typename VT>
+__global__ void k_set_out(ProdDev<PT, VT> *dst, int32_t *Cj, VT *Cx, void *Cp,
+                          int cp_bits) {
+  dst->Cj = Cj;
+  dst->Cx = Cx;
+  dst->Cp = Cp;
+  dst->cp_bits = cp_bits;
+}
+
+// One warp per B row: set *flag = 0 if some row is not strictly increasing
+// (the cursor sweep of the DENSE numeric class relies on sorted B rows).
+template <typename PT>
+__global__ void k_check_sorted_rows(const PT *Bp, const int32_t *Bj,
+                                    int64_t nb, int32_t *flag) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  bool bad = false;
+  for (int64_t r = warp; r < nb; r += nwarps) {
+    const int64_t b0 = Bp[r], b1 = Bp[r + 1];
+    for (int64_t q = b0 + lane; q + 1 < b1; q += 32)
+      if (Bj[q] >= Bj[q + 1]) bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) *flag = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Phase 0: mults per row and symbolic classes (one warp per row, shuffle
+// reduction), block-aggregated class counts.
+template <typename PT, typename VT>
+__global__ void __launch_bounds__(256) k_row_mults(
+    const ProdDev<PT, VT> *prods, const int64_t *base, int nprod, int64_t R,
+    int64_t *rowf, Sched *S) {
+  __shared__ unsigned long long s_cnt[NCLS];
+  __shared__ unsigned long long s_tot, s_up, s_ne;
+  __shared__ long long s_maxa;
+  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x == 0) s_tot = s_up = s_ne = 0, s_maxa = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long tot = 0, up = 0, ne = 0;
+  long long maxa = 0;
+  for (int64_t g = warp; g < R; g += nwarps) {
+    const int p = find_prod(base, nprod, g);
+    const int64_t r = g - base[p];
+    const PT *Ap = prods[p].Ap;
+    const int32_t *Aj = prods[p].Aj;
+    const PT *Bp = prods[p].Bp;
+    const int64_t a0 = Ap[r], a1 = Ap[r + 1];
+    int64_t f = 0;
+    for (int64_t q = a0 + lane; q < a1; q += 32) {
+      const int64_t k = Aj[q];
+      f += int64_t(Bp[k + 1]) - int64_t(Bp[k]);
+    }
+    f = warp_sum(f);
+    if (lane == 0) {
+      rowf[g] = f;
+      const int64_t n = prods[p].n;
+      const int c = sym_class(f, n);
+      if (c >= 0) {
+        atomicAdd(&s_cnt[c], 1ull);
+        ne += 1;
+      }
+      tot += f;
+      up += f < n ? f : n;
+      if (a1 - a0 > maxa) maxa = a1 - a0;
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&s_tot, tot);
+    atomicAdd(&s_up, up);
+    atomicAdd(&s_ne, ne);
+    atomicMax(&s_maxa, maxa);
+  }
+  __syncthreads();
+  if (threadIdx.x < NCLS && s_cnt[threadIdx.x])
+    atomicAdd((unsigned long long *)&S->cnt[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x == 0) {
+    atomicAdd((unsigned long long *)&S->total, s_tot);
+    atomicAdd((unsigned long long *)&S->upper, s_up);
+    atomicAdd((unsigned long long *)&S->nonempty, s_ne);
+    atomicMax((long long *)&S->max_a_row, s_maxa);
+  }
+}
+
+// Class offsets into the row list and the work-item prefix.
+static __global__ void k_sched_offsets(Sched *S) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    int64_t o = 0, it = 0;
+    for (int c = 0; c < NCLS; ++c) {
+      S->off[c] = o;
+      S->cur[c] = o;
+      o += S->cnt[c];
+      S->items[c] = it;
+      const int rpi = cls_rows_per_item(c);
+      it += (S->cnt[c] + rpi - 1) / rpi;
+    }
+    S->items[NCLS] = it;
+    S->work = 0;
+  }
+}
+
+// Scatter rows into the class lists.  mode 0: symbolic (class from rowf);
+// mode 1: numeric (class from rowc) which also writes the output row offsets
+// of each product and the largest A row among DENSE rows.
+template <typename PT, typename VT, int MODE>
+__global__ void __launch_bounds__(256) k_scatter(
+    ProdDev<PT, VT> *prods, const int64_t *base, int nprod, int64_t R,
+    const int64_t *rowf, const int32_t *rowc, const int64_t *cp, Sched *S,
+    uint64_t *list) {
+  __shared__ unsigned long long s_cnt[NCLS], s_base[NCLS];
+  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  int c = -1, p = 0;
+  int64_t r = 0;
+  unsigned long long my = 0;
+  if (g < R) {
+    p = find_prod(base, nprod, g);
+    r = g - base[p];
+    if (MODE == 0) {
+      c = sym_class(rowf[g], prods[p].n);
+    } else {
+      c = num_class(rowc[g]);
+      const int64_t off = cp[g] - cp[base[p]];
+      if (prods[p].cp_bits == 32)
+        ((int32_t *)prods[p].Cp)[r] = (int32_t)off;
+      else
+        ((int64_t *)prods[p].Cp)[r] = off;
+      if (r == prods[p].m - 1) {
+        const int64_t end = cp[g + 1] - cp[base[p]];
+        if (prods[p].cp_bits == 32)
+          ((int32_t *)prods[p].Cp)[r + 1] = (int32_t)end;
+        else
+          ((int64_t *)prods[p].Cp)[r + 1] = end;
+      }
+    }
+    if (c >= 0) my = atomicAdd(&s_cnt[c], 1ull);
+  }
+  __syncthreads();
+  if (threadIdx.x < NCLS) {
+    s_base[threadIdx.x] =
+        s_cnt[threadIdx.x]
+            ? atomicAdd((unsigned long long *)&S->cur[threadIdx.x],
+                        s_cnt[threadIdx.x])
+            : 0;
+  }
+  __syncthreads();
+  if (c >= 0) list[s_base[c] + my] = (uint64_t(p) << 40) | uint64_t(r);
+}
+
+// Products whose A has zero rows still need rowptr[0] = 0.
+template <typename PT, typename VT>
+__global__ void k_zero_rowptr(ProdDev<PT, VT> *prods, int nprod) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < nprod && prods[p].m == 0) {
+    if (prods[p].cp_bits == 32) ((int32_t *)prods[p].Cp)[0] = 0;
+    else ((int64_t *)prods[p].Cp)[0] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan of int32 row counts into int64 offsets
+// (reduce, scan of partials, final).  cp has R + 1 entries.
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+static __global__ void __launch_bounds__(kScanThreads)
+    k_scan_reduce(const int32_t *in, int64_t R, int64_t *partial) {
+  __shared__ int64_t tmp[kScanThreads / 32 + 1];
+  const int64_t t0 = int64_t(blockIdx.x) * kScanTile;
+  int64_t s = 0;
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t j = t0 + int64_t(i) * kScanThreads + threadIdx.x;
+    if (j < R) s += in[j];
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int64_t v = threadIdx.x < kScanThreads / 32 ? tmp[threadIdx.x] : 0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+// Single block: exclusive scan of nb partials in place; partial[nb] = total.
+static __global__ void __launch_bounds__(1024) k_scan_partials(int64_t *partial,
+                                                        int64_t nb) {
+  __shared__ int64_t tmp[33];
+  __shared__ int64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t b0 = 0; b0 < nb; b0 += 1024) {
+    const int64_t j = b0 + threadIdx.x;
+    const int64_t v = j < nb ? partial[j] : 0;
+    int64_t tot;
+    const int64_t ex = group_excl_scan<1024, int64_t>(v, tmp, 0, &tot);
+    if (j < nb) partial[j] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[nb] = carry;
+}
+
+// Also counts the numeric classes of the rows into *Snum.
+static __global__ void __launch_bounds__(kScanThreads)
+    k_scan_final(const int32_t *in, int64_t R, const int64_t *partial,
+                 int64_t nb, int64_t *out, Sched *Snum) {
+  __shared__ int64_t tmp[kScanThreads / 32 + 1];
+  __shared__ unsigned long long s_cnt[NCLS];
+  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t t0 = int64_t(blockIdx.x) * kScanTile;
+  // each thread owns kScanItems consecutive elements
+  const int64_t j0 = t0 + int64_t(threadIdx.x) * kScanItems;
+  int64_t v[kScanItems];
+  int64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (j0 + i < R) ? in[j0 + i] : 0;
+    s += v[i];
+    const int c = num_class(v[i]);
+    if (c >= 0) atomicAdd(&s_cnt[c], 1ull);
+  }
+  int64_t tot;
+  int64_t ex = group_excl_scan<kScanThreads, int64_t>(s, tmp, 0, &tot);
+  ex += partial[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (j0 + i < R) out[j0 + i] = ex;
+    ex += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[R] = partial[nb];
+  __syncthreads();
+  if (threadIdx.x < NCLS && s_cnt[threadIdx.x])
+    atomicAdd((unsigned long long *)&Snum->cnt[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+}  // namespace tspg

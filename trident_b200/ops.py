@@ -1,0 +1,237 @@
+"""Python host API over the C ABI (device operands as torch CUDA tensors).
+
+Function names follow the reference's operators: ``spgemm`` / ``sp_mma`` /
+``spadd`` are LocalMatrix::spgemm / sp_mma / spadd
+(include/KokkosWrap.hpp:60-66), ``spgeam`` is cusparse_spgeam
+(include/cusparse_helpers.cuh:799), ``gen_bitmask`` / ``intersect_bitmasks`` /
+``compress`` are SpaComm::gen_bitmask / intersect_bitmasks /
+SpaCommHandler::Compress (include/spacomm.cuh:29,126,962).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from ._lib import (ALLOC_FN, TSPG_COLS, TSPG_ENOMEM, TSPG_OK, TSPG_ROWS, TspgCsr,
+                   TspgCsrOut, TspgError, check, lib)
+from .csr import DeviceCSR
+
+
+def _stream_ptr(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+class _TorchAlloc:
+    """Allocator callback handing torch tensors to the library (kept alive here)."""
+
+    def __init__(self, device):
+        self.device = device
+        self.tensors = []
+        self.cb = ALLOC_FN(self._alloc)
+
+    def _alloc(self, user, nbytes, stream):
+        t = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
+        self.tensors.append(t)
+        return t.data_ptr()
+
+
+class Context:
+    """A library context: device, workspace pool (resident), budget."""
+
+    def __init__(self, device: int = 0, budget: int = 0):
+        torch.cuda.set_device(device)
+        self.device = device
+        h = C.c_void_p()
+        check(lib.tspg_ctx_create(device, budget, C.byref(h)), "tspg_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.tspg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mem(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        check(lib.tspg_ctx_mem(self.h, C.byref(a), C.byref(b)), "tspg_ctx_mem")
+        return a.value, b.value
+
+
+def _out_struct(nrows, ncols, rowptr, val_bits, col=None, val=None, capacity=0, alloc=None):
+    o = TspgCsrOut()
+    o.nrows, o.ncols = nrows, ncols
+    o.rowptr = rowptr.data_ptr()
+    o.rowptr_bits = 32 if rowptr.element_size() == 4 else 64
+    o.val_bits = val_bits
+    o.col = col.data_ptr() if col is not None else None
+    o.val = val.data_ptr() if val is not None else None
+    o.capacity = capacity
+    if alloc is not None:
+        o.alloc = alloc.cb
+    return o
+
+
+def _vdtype(bits):
+    return torch.float64 if bits == 64 else torch.float32
+
+
+class Plan:
+    """Symbolic result kept for numeric re-runs (cusparse_spgemm_reuse)."""
+
+    def __init__(self, ctx: Context, A: DeviceCSR, B: DeviceCSR, flags: int = 0, stream=None):
+        self.ctx = ctx
+        h = C.c_void_p()
+        nnz = C.c_int64()
+        a, b = A.abi(), B.abi()
+        check(lib.tspg_spgemm_symbolic(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b), flags,
+                                       C.byref(h), C.byref(nnz)), "tspg_spgemm_symbolic")
+        self.h = h
+        self.c_nnz = nnz.value
+        self.shape = (A.nrows, B.ncols)
+
+    def numeric(self, A: DeviceCSR, B: DeviceCSR, rowptr_bits: int = 64, stream=None) -> DeviceCSR:
+        m, n = self.shape
+        dev = A.rowptr.device
+        rp = torch.empty(m + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64, device=dev)
+        col = torch.empty(max(self.c_nnz, 1), dtype=torch.int32, device=dev)
+        val = torch.empty(max(self.c_nnz, 1), dtype=_vdtype(A.val_bits), device=dev)
+        o = _out_struct(m, n, rp, A.val_bits, col, val, self.c_nnz)
+        a, b = A.abi(), B.abi()
+        check(lib.tspg_spgemm_numeric(self.ctx.h, _stream_ptr(stream), self.h, C.byref(a), C.byref(b),
+                                      C.byref(o)), "tspg_spgemm_numeric")
+        return DeviceCSR(m, n, rp, col, val, nnz=self.c_nnz)
+
+    def close(self):
+        if self.h:
+            lib.tspg_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spgemm(ctx: Context, A: DeviceCSR, B: DeviceCSR, rowptr_bits: int = 64, flags: int = 0,
+           stream=None) -> DeviceCSR:
+    """C = A·B (LocalMatrix::spgemm, include/KokkosWrap.hpp:367-391)."""
+    p = Plan(ctx, A, B, flags, stream)
+    try:
+        return p.numeric(A, B, rowptr_bits, stream)
+    finally:
+        p.close()
+
+
+def spgemm_count(ctx: Context, A: DeviceCSR, B: DeviceCSR, stream=None):
+    """(mults, sum_i min(mults_i, ncols)) — the flop-count pass."""
+    mults, up = C.c_int64(), C.c_int64()
+    a, b = A.abi(), B.abi()
+    check(lib.tspg_spgemm_count(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b), C.byref(mults),
+                                C.byref(up)), "tspg_spgemm_count")
+    return mults.value, up.value
+
+
+def _finish(o: TspgCsrOut, rp, alloc: _TorchAlloc, val_bits: int) -> DeviceCSR:
+    nnz = int(o.nnz)
+    if nnz == 0:
+        col = torch.empty(1, dtype=torch.int32, device=rp.device)
+        val = torch.empty(1, dtype=_vdtype(val_bits), device=rp.device)
+        return DeviceCSR(int(o.nrows), int(o.ncols), rp, col, val, nnz=0)
+    colbuf, valbuf = alloc.tensors[-2], alloc.tensors[-1]
+    col = colbuf.view(torch.int32)[:nnz]
+    val = valbuf.view(_vdtype(val_bits))[:nnz]
+    return DeviceCSR(int(o.nrows), int(o.ncols), rp, col, val, nnz=nnz)
+
+
+def sp_mma(ctx: Context, A: DeviceCSR, B: DeviceCSR, C_in: DeviceCSR | None, rowptr_bits: int = 64,
+           flags: int = 0, stream=None) -> DeviceCSR:
+    """C_out = C_in + A·B (LocalMatrix::sp_mma / sp_mma_hybrid)."""
+    m, n = A.nrows, B.ncols
+    rp = torch.empty(m + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64, device=A.rowptr.device)
+    alloc = _TorchAlloc(A.rowptr.device)
+    o = _out_struct(m, n, rp, A.val_bits, alloc=alloc)
+    a, b = A.abi(), B.abi()
+    cin = C_in.abi() if C_in is not None else None
+    check(lib.tspg_spgemm_acc(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b),
+                              C.byref(cin) if cin is not None else None, C.byref(o), flags),
+          "tspg_spgemm_acc")
+    return _finish(o, rp, alloc, A.val_bits)
+
+
+def spadd(ctx: Context, A: DeviceCSR, B: DeviceCSR, rowptr_bits: int = 64, stream=None) -> DeviceCSR:
+    """C = A + B, union pattern (cusparse_spgeam / LocalMatrix::spadd)."""
+    m, n = A.nrows, A.ncols
+    rp = torch.empty(m + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64, device=A.rowptr.device)
+    alloc = _TorchAlloc(A.rowptr.device)
+    o = _out_struct(m, n, rp, A.val_bits, alloc=alloc)
+    a, b = A.abi(), B.abi()
+    check(lib.tspg_spadd(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b), C.byref(o)), "tspg_spadd")
+    return _finish(o, rp, alloc, A.val_bits)
+
+
+spgeam = spadd
+
+
+def gen_bitmask(ctx: Context, ptr: torch.Tensor, n: int, stream=None) -> torch.Tensor:
+    """Bit i of the mask = segment i of ptr non-empty (SpaComm::gen_bitmask, MASK_SIZE 8)."""
+    out = torch.empty(max((n + 7) // 8, 1), dtype=torch.uint8, device=ptr.device)
+    bits = 32 if ptr.element_size() == 4 else 64
+    check(lib.tspg_bitmask_gen(ctx.h, _stream_ptr(stream), ptr.data_ptr(), bits, n, out.data_ptr()),
+          "tspg_bitmask_gen")
+    return out[: (n + 7) // 8]
+
+
+def intersect_bitmasks(ctx: Context, a: torch.Tensor, b: torch.Tensor, out: torch.Tensor | None = None,
+                       stream=None) -> torch.Tensor:
+    n = a.numel()
+    out = torch.empty_like(a) if out is None else out
+    check(lib.tspg_bitmask_and(ctx.h, _stream_ptr(stream), a.data_ptr(), b.data_ptr(), n, out.data_ptr()),
+          "tspg_bitmask_and")
+    return out
+
+
+def packed_bytes(nnz: int, ptr_len: int, val_bits: int = 64, ptr_bits: int = 32) -> int:
+    return int(lib.tspg_packed_bytes(nnz, ptr_len, val_bits, ptr_bits))
+
+
+def compress(ctx: Context, M: DeviceCSR, mask: torch.Tensor, major: int = TSPG_ROWS,
+             out: torch.Tensor | None = None, stream=None):
+    """Pack one tile by its segment mask; returns (wire buffer, kept nnz)."""
+    length = M.nrows if major == TSPG_ROWS else M.ncols
+    cap = packed_bytes(M.nnz, length, M.val_bits, M.rowptr_bits)
+    if out is None:
+        out = torch.empty(max(cap, 16), dtype=torch.uint8, device=M.rowptr.device)
+    kept = C.c_int64()
+    m = M.abi()
+    check(lib.tspg_pack(ctx.h, _stream_ptr(stream), C.byref(m), major, mask.data_ptr(), out.data_ptr(),
+                        out.numel(), None, C.byref(kept)), "tspg_pack")
+    return out, kept.value
+
+
+def unpack(buf: torch.Tensor, nrows: int, ncols: int, nnz: int, major: int = TSPG_ROWS,
+           val_bits: int = 64, ptr_bits: int = 32) -> DeviceCSR:
+    """View a packed tile as a CSX (TileHolder::form_mmiocsx); shares buf's memory."""
+    v = TspgCsr()
+    check(lib.tspg_unpack(buf.data_ptr(), nrows, ncols, major, nnz, val_bits, ptr_bits, C.byref(v)),
+          "tspg_unpack")
+    base = buf.data_ptr()
+    length = nrows if major == TSPG_ROWS else ncols
+    vb, pb = val_bits // 8, ptr_bits // 8
+    val = buf[0: nnz * vb].view(_vdtype(val_bits))
+    col = buf[v.col - base: v.col - base + nnz * 4].view(torch.int32)
+    off = v.rowptr - base
+    rp = buf[off: off + (length + 1) * pb].view(torch.int32 if ptr_bits == 32 else torch.int64)
+    return DeviceCSR(nrows, ncols, rp, col, val, nnz=nnz)
+
+
+__all__ = ["Context", "Plan", "spgemm", "spgemm_count", "sp_mma", "spadd", "spgeam", "gen_bitmask",
+           "intersect_bitmasks", "compress", "unpack", "packed_bytes", "TSPG_ROWS", "TSPG_COLS",
+           "TspgError", "TSPG_OK", "TSPG_ENOMEM"]
