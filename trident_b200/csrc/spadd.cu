@@ -45,12 +45,20 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Output rank of a column x of the union row: |{a < x}| + |{b < x}| minus
+// the columns below x present in both rows.  The fill walks A's row in warp
+// chunks, flags A entries that also occur in B (binary search), keeps the
+// running exclusive count of those flags in dpre[] (one int per A entry) and
+// writes every A entry; B entries absent from A then look their rank up
+// through dpre at their lower bound in A.
 template <typename PTA, typename PTB, typename VT>
 __global__ void __launch_bounds__(256)
     k_spadd_fill(int64_t m, const PTA *Ap, const int32_t *Aj, const VT *Ax,
                  const PTB *Bp, const int32_t *Bj, const VT *Bx,
-                 const int64_t *cp, void *Cp, int cp_bits, int32_t *Cj, VT *Cx) {
+                 const int64_t *cp, void *Cp, int cp_bits, int32_t *Cj, VT *Cx,
+                 int32_t *dpre) {
   const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t r = warp; r < m; r += nwarps) {
@@ -64,23 +72,40 @@ __global__ void __launch_bounds__(256)
         else ((int64_t *)Cp)[m] = cp[m];
       }
     }
-    for (int64_t p = a0 + lane; p < a1; p += 32) {
-      const int32_t x = __ldg(Aj + p);
-      const int64_t q = lower_bound_row<int>(Bj, b0, b1, x);
-      VT v = __ldg(Ax + p);
-      if (q < b1 && __ldg(Bj + q) == x) v += __ldg(Bx + q);
-      const int64_t pos = o + (p - a0) + (q - b0);
-      Cj[pos] = x;
-      Cx[pos] = v;
+    int running = 0;
+    for (int64_t base = a0; base < a1; base += 32) {
+      const int64_t p = base + lane;
+      bool dup = false;
+      int32_t x = 0;
+      int64_t q = b0;
+      if (p < a1) {
+        x = __ldg(Aj + p);
+        q = lower_bound_row<int>(Bj, b0, b1, x);
+        dup = q < b1 && __ldg(Bj + q) == x;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, dup);
+      const int pre = running + __popc(bal & below);
+      if (p < a1) {
+        dpre[p] = pre;
+        VT v = __ldg(Ax + p);
+        if (dup) v += __ldg(Bx + q);
+        const int64_t pos = o + (p - a0) + (q - b0) - pre;
+        Cj[pos] = x;
+        Cx[pos] = v;
+      }
+      running += __popc(bal);
     }
+    __syncwarp();
     for (int64_t q = b0 + lane; q < b1; q += 32) {
       const int32_t x = __ldg(Bj + q);
       const int64_t p = lower_bound_row<int>(Aj, a0, a1, x);
       if (p < a1 && __ldg(Aj + p) == x) continue;
-      const int64_t pos = o + (q - b0) + (p - a0);
+      const int common = p < a1 ? dpre[p] : running;
+      const int64_t pos = o + (q - b0) + (p - a0) - common;
       Cj[pos] = x;
       Cx[pos] = __ldg(Bx + q);
     }
+    __syncwarp();
   }
 }
 
@@ -89,11 +114,12 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                       const tspg_csr *B, tspg_csr_out *C) {
   const int64_t m = A->nrows;
   Scratch sc(ctx, s);
-  int32_t *rowc;
+  int32_t *rowc, *dpre;
   int64_t *cp, *partial;
   const int64_t nb = (m + kScanTile - 1) / kScanTile;
   Sched *dummy;
   TSPG_TRY(sc.get(&rowc, m));
+  TSPG_TRY(sc.get(&dpre, A->nnz));
   TSPG_TRY(sc.get(&cp, m + 1));
   TSPG_TRY(sc.get(&partial, nb + 1));
   TSPG_TRY(sc.get(&dummy, 1));
@@ -130,7 +156,7 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   }
   k_spadd_fill<PTA, PTB, VT><<<grid, 256, 0, s>>>(
       m, (const PTA *)A->rowptr, A->col, (const VT *)A->val, (const PTB *)B->rowptr,
-      B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val);
+      B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val, dpre);
   ctx->launches += 1;
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
