@@ -84,6 +84,8 @@ def _load() -> C.CDLL:
         "tspg_ctx_stats": (i32, [vp, P(i64)]),
         "tspg_ctx_phase_timing": (i32, [vp, i32]),
         "tspg_ctx_phase_ms": (i32, [vp, P(C.c_float), P(C.c_float)]),
+        "tspg_ctx_class_profile": (i32, [vp, i32]),
+        "tspg_ctx_class_cycles": (i32, [vp, P(C.c_uint64)]),
         "tspg_batch_create": (i32, [vp, P(vp)]),
         "tspg_batch_destroy": (i32, [vp]),
         "tspg_batch_clear": (i32, [vp]),

@@ -220,14 +220,15 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       k_sched_offsets<<<1, 32, 0, s>>>(b->sched);
       k_scatter<PT, VT, 0><<<(unsigned)((R + 255) / 256), 256, 0, s>>>(
           prods, b->d_base, nprod, R, b->rowf, b->rowc, b->cp, b->sched, b->list);
-      PhaseArgs pa{b->d_base, b->sched, b->list, b->rowf, b->rowc, b->cp, nullptr, 0, errw};
+      PhaseArgs pa{b->d_base, b->sched, b->list, b->rowf, b->rowc, b->cp, nullptr, 0, errw,
+                   ctx->d_prof};
       phase_mark(ctx, 0, 0, s);
       k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 0, 1, s);
       k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(b->rowc, R, b->partial);
       k_scan_partials<<<1, 1024, 0, s>>>(b->partial, nb);
       k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(b->rowc, R, b->partial, nb, b->cp,
-                                                         b->sched + 1);
+                                                         b->sched + 1, b->rowf);
     }
     k_gather_offsets<<<(nprod + 256) / 256, 256, 0, s>>>(b->cp, b->d_base, nprod, b->offs);
     b->g1_kernels = 1 + (!(flags & TSPG_F_B_SORTED) && b->RB > 0) + (R > 0 ? 7 : 0);
@@ -287,7 +288,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       k_scatter<PT, VT, 1><<<(unsigned)((R + 255) / 256), 256, 0, s>>>(
           prods, b->d_base, nprod, R, b->rowf, b->rowc, b->cp, b->sched + 1, b->list);
       PhaseArgs pa{b->d_base, b->sched + 1, b->list, b->rowf, b->rowc, b->cp,
-                   b->curbuf, b->cur_stride, errw};
+                   b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + 14 : nullptr};
       phase_mark(ctx, 1, 0, s);
       k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 1, 1, s);

@@ -133,7 +133,7 @@ static int pack_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *M,
     k_pack_counts<PT><<<(unsigned)((len + 255) / 256), 256, 0, s>>>(ptr, len, mask, cnt);
     k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(cnt, len, partial);
     k_scan_partials<<<1, 1024, 0, s>>>(partial, nb);
-    k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(cnt, len, partial, nb, newp, dummy);
+    k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(cnt, len, partial, nb, newp, dummy, nullptr);
     ctx->launches += 4;
   }
   ctx->launches += 1;

@@ -117,6 +117,7 @@ extern "C" int tspg_ctx_destroy(tspg_ctx *ctx) {
   cudaDeviceSynchronize();
   for (auto &e : ctx->ev)
     if (e) cudaEventDestroy(e);
+  if (ctx->d_prof) cudaFree(ctx->d_prof);
   for (auto &kv : ctx->live) cudaFree(kv.first);
   ctx->live.clear();
   if (ctx->h_words) cudaFreeHost(ctx->h_words);
@@ -167,5 +168,25 @@ extern "C" int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms,
   }
   if (symbolic_ms) *symbolic_ms = a;
   if (numeric_ms) *numeric_ms = b;
+  return TSPG_OK;
+}
+
+extern "C" int tspg_ctx_class_profile(tspg_ctx *ctx, int enable) {
+  if (!ctx) return TSPG_EINVAL;
+  TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (enable && !ctx->d_prof)
+    TSPG_CUDA(ctx, cudaMalloc((void **)&ctx->d_prof, 2 * 14 * sizeof(unsigned long long)));
+  if (enable) TSPG_CUDA(ctx, cudaMemset(ctx->d_prof, 0, 2 * 14 * sizeof(unsigned long long)));
+  if (!enable && ctx->d_prof) {
+    cudaFree(ctx->d_prof);
+    ctx->d_prof = nullptr;
+  }
+  return TSPG_OK;
+}
+
+extern "C" int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out28) {
+  if (!ctx || !ctx->d_prof || !out28) return TSPG_EINVAL;
+  TSPG_CUDA(ctx, cudaDeviceSynchronize());
+  TSPG_CUDA(ctx, cudaMemcpy(out28, ctx->d_prof, 28 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return TSPG_OK;
 }

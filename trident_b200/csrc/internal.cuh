@@ -30,6 +30,8 @@ struct tspg_ctx {
   bool phase_timing = false;   // record events around the persistent phases
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   bool ev_sym = false, ev_num = false;
+  // per-class cycle accounting of the persistent phases: [phase][2 * 7]
+  unsigned long long *d_prof = nullptr;
 };
 
 namespace tspg {
@@ -131,15 +133,19 @@ __device__ __forceinline__ T warp_scan_incl(T v) {
   return v;
 }
 
-// Synchronise a group of G threads (G = 32, 1024, or a named-barrier group).
+// Synchronise a group of G threads.  G = 32: the warp.  G = 256 / 128: named
+// barriers 1-4 / 5-12, disjoint so that 256- and 128-thread groups of one CTA
+// can be active at the same time.  Any other G is a whole block.
 template <int G>
 __device__ __forceinline__ void group_sync(int gid) {
   if constexpr (G == 32) {
     __syncwarp();
-  } else if constexpr (G >= 1024) {
-    __syncthreads();
-  } else {
+  } else if constexpr (G == 256) {
     asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(G) : "memory");
+  } else if constexpr (G == 128) {
+    asm volatile("bar.sync %0, %1;" ::"r"(gid + 5), "r"(G) : "memory");
+  } else {
+    __syncthreads();
   }
 }
 
@@ -177,6 +183,32 @@ __device__ __forceinline__ T group_sum(T v, T *tmp, int gid) {
   T total;
   group_excl_scan<G, T>(v, tmp, gid, &total);
   return total;
+}
+
+// Min and max across a group (tmp: 2 * (G/32) + 2 ints of group-private smem).
+template <int G>
+__device__ __forceinline__ void group_minmax(int &mn, int &mx, int *tmp, int gid) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if constexpr (G > 32) {
+    constexpr int NW = G / 32;
+    const int w = (threadIdx.x % G) >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+      tmp[w] = mn;
+      tmp[NW + w] = mx;
+    }
+    group_sync<G>(gid);
+    mn = tmp[0];
+    mx = tmp[NW];
+    for (int i = 1; i < NW; ++i) {
+      mn = min(mn, tmp[i]);
+      mx = max(mx, tmp[NW + i]);
+    }
+    group_sync<G>(gid);
+  }
 }
 
 __device__ __forceinline__ void set_error(int64_t *err, int code) {

@@ -131,7 +131,7 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                                                  (const PTB *)B->rowptr, B->col, rowc);
     k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial);
     k_scan_partials<<<1, 1024, 0, s>>>(partial, nb);
-    k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial, nb, cp, dummy);
+    k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial, nb, cp, dummy, nullptr);
     ctx->launches += 4;
   }
   TSPG_CUDA(ctx, cudaGetLastError());

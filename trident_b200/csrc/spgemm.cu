@@ -131,14 +131,14 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
     k_scatter<PT, VT, 0><<<grid_for(m, 256, INT32_MAX), 256, 0, s>>>(
         prods, P->base, 1, m, P->rowf, P->rowc, P->cp, P->sched, P->list);
     PhaseArgs pa{P->base, P->sched, P->list, P->rowf, P->rowc, P->cp,
-                 nullptr, 0, ctx->d_words + kErrWord};
+                 nullptr, 0, ctx->d_words + kErrWord, ctx->d_prof};
     phase_mark(ctx, 0, 0, s);
     k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
     phase_mark(ctx, 0, 1, s);
     k_scan_reduce<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial);
     k_scan_partials<<<1, 1024, 0, s>>>(P->partial, P->nb);
     k_scan_final<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial,
-                                                          P->nb, P->cp, P->sched + 1);
+                                                          P->nb, P->cp, P->sched + 1, P->rowf);
   }
   TSPG_CUDA(ctx, cudaGetLastError());
   ctx->launches += 1 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 7 : 0);
@@ -180,7 +180,8 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
   k_scatter<PT, VT, 1><<<grid_for(m, 256, INT32_MAX), 256, 0, s>>>(
       prods, P->base, 1, m, P->rowf, P->rowc, P->cp, P->sched + 1, P->list);
   PhaseArgs pa{P->base, P->sched + 1, P->list, P->rowf, P->rowc, P->cp,
-               P->curbuf, P->cur_stride, ctx->d_words + kErrWord};
+               P->curbuf, P->cur_stride, ctx->d_words + kErrWord,
+               ctx->d_prof ? ctx->d_prof + 14 : nullptr};
   phase_mark(ctx, 1, 0, s);
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
   phase_mark(ctx, 1, 1, s);

@@ -29,16 +29,25 @@
 namespace tspg {
 
 constexpr int kThreads = 1024;
-constexpr int kDynSmem = 196608;  // 192 KiB per CTA, one CTA per SM
-constexpr int NCLS = 5;
-enum { CLS_DENSE = 0, CLS_G1024 = 1, CLS_G256 = 2, CLS_G128 = 3, CLS_G32 = 4 };
-__host__ __device__ constexpr int cls_group(int c) {
-  return c <= CLS_G1024 ? 1024 : c == CLS_G256 ? 256 : c == CLS_G128 ? 128 : 32;
-}
-// rows handled by one work item of each class
-__host__ __device__ constexpr int cls_rows_per_item(int c) {
-  return c <= CLS_G1024 ? 1 : c == CLS_G256 ? 4 : c == CLS_G128 ? 8 : 64;
-}
+constexpr int kTableSmem = 196608;              // hash tables / dense window
+constexpr int kCountSmem = 16384;               // radix-sort digit counters
+constexpr int kDynSmem = kTableSmem + kCountSmem;  // one CTA per SM
+
+// Row classes, heaviest first.  The first four are worked by the whole CTA
+// (items fetched by one thread); G256 / G128 / G32 rows are fetched by each
+// group on its own, so groups never wait for one another.
+constexpr int NCLS = 7;
+enum {
+  CLS_DENSE0 = 0,  // DENSE rows with >= 2^20 products
+  CLS_DENSE1 = 1,  // DENSE rows with >= 2^17 products
+  CLS_DENSE2 = 2,  // other DENSE rows
+  CLS_G1024 = 3,
+  CLS_G256 = 4,
+  CLS_G128 = 5,
+  CLS_G32 = 6
+};
+constexpr int kCtaClasses = 4;  // classes [0, 4) are CTA-level
+__host__ __device__ constexpr bool cls_dense(int c) { return c <= CLS_DENSE2; }
 
 // Class limits (symbolic: on min(mults, ncols); numeric: on the row's nnz).
 // Symbolic tables hold int32 keys (128 KiB per CTA), numeric tables hold
@@ -53,8 +62,12 @@ constexpr int kNumT32 = 512, kNumT128 = 2048, kNumT256 = 4096,
               kNumT1024 = 16384;
 constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory
-constexpr int64_t kDenseBits = int64_t(kDynSmem) * 8;  // symbolic bitmap
+constexpr int64_t kDenseBits = int64_t(kTableSmem) * 8;  // symbolic bitmap
+constexpr int kBitonicMax = 64;          // rows up to this size sort bitonic
 
+__host__ __device__ inline int dense_sub(int64_t f) {
+  return f >= (int64_t(1) << 20) ? CLS_DENSE0 : f >= (int64_t(1) << 17) ? CLS_DENSE1 : CLS_DENSE2;
+}
 __host__ __device__ inline int sym_class(int64_t f, int64_t n) {
   const int64_t fe = f < n ? f : n;
   if (f == 0) return -1;
@@ -62,15 +75,15 @@ __host__ __device__ inline int sym_class(int64_t f, int64_t n) {
   if (fe <= kSymLim128) return CLS_G128;
   if (fe <= kSymLim256) return CLS_G256;
   if (fe <= kSymLim1024) return CLS_G1024;
-  return CLS_DENSE;
+  return dense_sub(f);
 }
-__host__ __device__ inline int num_class(int64_t c) {
+__host__ __device__ inline int num_class(int64_t c, int64_t f) {
   if (c == 0) return -1;
   if (c <= kNumLim32) return CLS_G32;
   if (c <= kNumLim128) return CLS_G128;
   if (c <= kNumLim256) return CLS_G256;
   if (c <= kNumLim1024) return CLS_G1024;
-  return CLS_DENSE;
+  return dense_sub(f);
 }
 
 template <typename PT, typename VT>
@@ -95,8 +108,8 @@ struct Sched {
   int64_t cnt[NCLS];
   int64_t off[NCLS];
   int64_t cur[NCLS];
-  int64_t items[NCLS + 1];
-  unsigned long long work;
+  unsigned long long next[NCLS];  // per-class row counters of the group-level classes
+  unsigned long long work;        // item counter of the CTA-level classes
   int64_t total;      // sum of mults (symbolic) or of nnz (numeric)
   int64_t upper;      // sum of min(mults, ncols)
   int64_t max_a_row;  // longest A row (sizes the DENSE cursor scratch)
@@ -241,19 +254,16 @@ __global__ void __launch_bounds__(256) k_row_mults(
   }
 }
 
-// Class offsets into the row list and the work-item prefix.
+// Class offsets into the row list; resets the work counters.
 static __global__ void k_sched_offsets(Sched *S) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    int64_t o = 0, it = 0;
+    int64_t o = 0;
     for (int c = 0; c < NCLS; ++c) {
       S->off[c] = o;
       S->cur[c] = o;
+      S->next[c] = 0;
       o += S->cnt[c];
-      S->items[c] = it;
-      const int rpi = cls_rows_per_item(c);
-      it += (S->cnt[c] + rpi - 1) / rpi;
     }
-    S->items[NCLS] = it;
     S->work = 0;
   }
 }
@@ -279,7 +289,7 @@ __global__ void __launch_bounds__(256) k_scatter(
     if (MODE == 0) {
       c = sym_class(rowf[g], prods[p].n);
     } else {
-      c = num_class(rowc[g]);
+      c = num_class(rowc[g], rowf[g]);
       const int64_t off = cp[g] - cp[base[p]];
       if (prods[p].cp_bits == 32)
         ((int32_t *)prods[p].Cp)[r] = (int32_t)off;
@@ -366,7 +376,7 @@ static __global__ void __launch_bounds__(1024) k_scan_partials(int64_t *partial,
 // Also counts the numeric classes of the rows into *Snum.
 static __global__ void __launch_bounds__(kScanThreads)
     k_scan_final(const int32_t *in, int64_t R, const int64_t *partial,
-                 int64_t nb, int64_t *out, Sched *Snum) {
+                 int64_t nb, int64_t *out, Sched *Snum, const int64_t *rowf) {
   __shared__ int64_t tmp[kScanThreads / 32 + 1];
   __shared__ unsigned long long s_cnt[NCLS];
   if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
@@ -380,8 +390,7 @@ static __global__ void __launch_bounds__(kScanThreads)
   for (int i = 0; i < kScanItems; ++i) {
     v[i] = (j0 + i < R) ? in[j0 + i] : 0;
     s += v[i];
-    const int c = num_class(v[i]);
-    if (c >= 0) atomicAdd(&s_cnt[c], 1ull);
+    if (rowf && v[i] > 0) atomicAdd(&s_cnt[num_class(v[i], rowf[j0 + i])], 1ull);
   }
   int64_t tot;
   int64_t ex = group_excl_scan<kScanThreads, int64_t>(s, tmp, 0, &tot);

@@ -1,8 +1,16 @@
 // spgemm_phase.cuh — the persistent symbolic / numeric kernels.
 //
-// One 1024-thread CTA per SM (192 KiB of dynamic shared memory) pulls work
-// items from a device counter; an item is one DENSE or G1024 row, 4 G256
-// rows, 8 G128 rows or 64 G32 rows.  Item numbers run heaviest class first.
+// One 1024-thread CTA per SM (208 KiB of dynamic shared memory).  Work is
+// taken in two stages:
+//   1. CTA-level rows (DENSE0..2 heaviest first, then G1024): thread 0 takes
+//      the next row index from a device counter, the whole CTA works on it.
+//   2. When those run out, the CTA splits into four 256-thread groups that
+//      take G256 rows from their own counter; a group that runs out splits
+//      into two 128-thread groups (G128 rows), which split into warps (G32
+//      rows).  Groups never wait for each other: their shared-memory slices
+//      and digit counters nest (a 128-group's slice lies inside its 256-group's
+//      slice, a warp's inside its 128-group's) and they use disjoint named
+//      barriers.
 #pragma once
 
 #include "spgemm_kernels.cuh"
@@ -28,6 +36,58 @@ __device__ __forceinline__ void for_products(const int32_t *__restrict__ Aj,
     for (int64_t q = __ldg(Bp + k) + sl; q < b1; q += S) {
       if constexpr (NUM) f(__ldg(Bj + q), a * __ldg(Bx + q));
       else f(__ldg(Bj + q), VT(0));
+    }
+  }
+}
+
+// Balanced product loop for one row by a group of G threads.  Pass 1: as
+// for_products, but an A entry whose B row is longer than the fair share of a
+// sub-group (f / #sub-groups) is appended to `lst` (group-private shared
+// memory, `cap` slots, count in *nl) instead; pass 2 walks each listed B row
+// with all G threads, so a hub row of B never leaves the group waiting on
+// one warp.  When the list is full the entry is done in pass 1.
+template <int G, bool NUM, typename PT, typename VT, typename F>
+__device__ __forceinline__ void for_products_balanced(
+    const int32_t *__restrict__ Aj, const VT *__restrict__ Ax,
+    const PT *__restrict__ Bp, const int32_t *__restrict__ Bj,
+    const VT *__restrict__ Bx, int64_t a0, int64_t a1, int64_t f, int S,
+    int lane, int gid, int *lst, int *nl, int cap, F &&fn) {
+  const int sub = lane / S, sl = lane - sub * S, nsub = G / S;
+  const int64_t thr = nsub > 1 ? max(int64_t(4 * S), f / nsub) : INT64_MAX;
+  const unsigned submask =
+      S >= 32 ? 0xffffffffu : (((1u << S) - 1u) << (((lane & 31) / S) * S));
+  if (lane == 0) *nl = 0;
+  group_sync<G>(gid);
+  for (int64_t p = a0 + sub; p < a1; p += nsub) {
+    const int64_t k = __ldg(Aj + p);
+    const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+    if (b1 - b0 > thr) {
+      int slot = 0;
+      if (sl == 0) slot = atomicAdd(nl, 1);
+      slot = __shfl_sync(submask, slot, (lane & 31) - sl);
+      if (slot < cap) {
+        if (sl == 0) lst[slot] = int(p - a0);
+        continue;
+      }
+    }
+    VT a = VT(0);
+    if constexpr (NUM) a = __ldg(Ax + p);
+    for (int64_t q = b0 + sl; q < b1; q += S) {
+      if constexpr (NUM) fn(__ldg(Bj + q), a * __ldg(Bx + q));
+      else fn(__ldg(Bj + q), VT(0));
+    }
+  }
+  group_sync<G>(gid);
+  const int n = min(*nl, cap);
+  for (int i = 0; i < n; ++i) {
+    const int64_t p = a0 + lst[i];
+    const int64_t k = __ldg(Aj + p);
+    VT a = VT(0);
+    if constexpr (NUM) a = __ldg(Ax + p);
+    const int64_t b1 = __ldg(Bp + k + 1);
+    for (int64_t q = __ldg(Bp + k) + lane; q < b1; q += G) {
+      if constexpr (NUM) fn(__ldg(Bj + q), a * __ldg(Bx + q));
+      else fn(__ldg(Bj + q), VT(0));
     }
   }
 }
@@ -78,65 +138,82 @@ struct PhaseArgs {
   int32_t *curbuf;     // per-CTA cursor scratch for DENSE rows with long A rows
   int64_t cur_stride;  // entries per CTA in curbuf
   int64_t *err;
+  unsigned long long *prof;  // optional: [class] cycles, [NCLS + class] rows
+};
+
+// Optional per-class accounting (SM cycles spent in each row class).
+__device__ __forceinline__ void prof_add(const PhaseArgs &A, int cls, long long t0,
+                                         bool leader) {
+  if (A.prof && leader) {
+    atomicAdd(A.prof + cls, (unsigned long long)(clock64() - t0));
+    atomicAdd(A.prof + NCLS + cls, 1ull);
+  }
+}
+
+struct RowRef {
+  int p;
+  int64_t r, g;
+};
+
+__device__ __forceinline__ RowRef decode_row(const PhaseArgs &A, int64_t idx) {
+  const uint64_t e = A.list[idx];
+  RowRef rr;
+  rr.p = int(e >> 40);
+  rr.r = int64_t(e & ((uint64_t(1) << 40) - 1));
+  rr.g = A.base[rr.p] + rr.r;
+  return rr;
+}
+
+// Group-private shared scratch handed to the row functions.
+struct GroupMem {
+  int64_t *tmp;   // scan scratch (33 words)
+  int *itmp;      // min/max scratch
+  int *lst;       // deferred long B rows
+  int *nl;        // their count
+  int cap;        // list capacity
+  uint16_t *cnt;  // radix digit counters
 };
 
 // ---------------------------------------------------------------- symbolic
 
 template <int G, int TMAX, typename PT, typename VT>
-__device__ void sym_hash_rows(const ProdDev<PT, VT> *prods,
-                              const PhaseArgs &A, int64_t first, int64_t last,
-                              unsigned char *smem, int64_t *scan_tmp) {
-  constexpr int NG = kThreads / G;
-  constexpr int RPI = cls_rows_per_item(
-      G == 1024 ? CLS_G1024 : G == 256 ? CLS_G256 : G == 128 ? CLS_G128 : CLS_G32);
-  static_assert(NG * TMAX * 4 <= kDynSmem, "symbolic table exceeds shared memory");
-  const int gid = threadIdx.x / G, lane = threadIdx.x % G;
-  int *keys = (int *)smem + gid * TMAX;
-  int64_t *tmp = scan_tmp + gid * 33;
-  for (int64_t idx = first + gid; idx < last && idx < first + RPI; idx += NG) {
-    const uint64_t e = A.list[idx];
-    const int p = int(e >> 40);
-    const int64_t r = int64_t(e & ((uint64_t(1) << 40) - 1));
-    const int64_t g = A.base[p] + r;
-    const ProdDev<PT, VT> &P = prods[p];
-    const int64_t f = A.rowf[g];
-    const int64_t n = P.n;
-    const int64_t fe = f < n ? f : n;
-    uint32_t T = pow2_at_least(2 * fe, 32);
-    if (T > TMAX) T = TMAX;
-    const int logT = ilog2_pow2(T);
-    const uint32_t mask = T - 1;
-    for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
-    group_sync<G>(gid);
-    const int64_t a0 = P.Ap[r], a1 = P.Ap[r + 1];
-    const int S = subgroup_width(f, a1 - a0, G);
-    int cnt = 0;
-    for_products<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, S,
-                                   lane, [&](int32_t col, VT) {
-                                     cnt += sym_insert(keys, col, logT, mask,
-                                                       A.err);
-                                   });
-    group_sync<G>(gid);
-    const int64_t total = group_sum<G, int64_t>(int64_t(cnt), tmp, gid);
-    if (lane == 0) A.rowc[g] = int32_t(total);
-    group_sync<G>(gid);
-  }
+__device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                             int64_t idx, int *keys, const GroupMem &gm, int gid,
+                             int lane) {
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
+  const int64_t f = A.rowf[rr.g];
+  const int64_t n = P.n;
+  const int64_t fe = f < n ? f : n;
+  uint32_t T = pow2_at_least(2 * fe, 32);
+  if (T > TMAX) T = TMAX;
+  const int logT = ilog2_pow2(T);
+  const uint32_t mask = T - 1;
+  for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
+  group_sync<G>(gid);
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int S = subgroup_width(f, a1 - a0, G);
+  int cnt = 0;
+  for_products_balanced<G, false, PT, VT>(
+      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane, gid, gm.lst, gm.nl, gm.cap,
+      [&](int32_t col, VT) { cnt += sym_insert(keys, col, logT, mask, A.err); });
+  group_sync<G>(gid);
+  const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
+  if (lane == 0) A.rowc[rr.g] = int32_t(total);
+  group_sync<G>(gid);
 }
 
 template <typename PT, typename VT>
 __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
-                              int64_t idx, unsigned char *smem,
-                              int64_t *scan_tmp) {
+                              int64_t idx, unsigned char *smem, const GroupMem &gm) {
+  int64_t *scan_tmp = gm.tmp;
   const int tid = threadIdx.x;
   uint32_t *bm = (uint32_t *)smem;
-  const uint64_t e = A.list[idx];
-  const int p = int(e >> 40);
-  const int64_t r = int64_t(e & ((uint64_t(1) << 40) - 1));
-  const int64_t g = A.base[p] + r;
-  const ProdDev<PT, VT> &P = prods[p];
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t n = P.n;
-  const int64_t a0 = P.Ap[r], a1 = P.Ap[r + 1];
-  const int S = subgroup_width(A.rowf[g], a1 - a0, 32);
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int S = subgroup_width(A.rowf[rr.g], a1 - a0, 32);
   const int64_t W = n < kDenseBits ? n : kDenseBits;
   int64_t total = 0;
   for (int64_t w0 = 0; w0 < n; w0 += W) {
@@ -144,8 +221,9 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     const int64_t nw = (w1 - w0 + 31) >> 5;
     for (int64_t i = tid; i < nw; i += kThreads) bm[i] = 0u;
     __syncthreads();
-    for_products<kThreads, false, PT, VT>(
-        P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, S, tid, [&](int32_t col, VT) {
+    for_products_balanced<kThreads, false, PT, VT>(
+        P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl, gm.cap,
+        [&](int32_t col, VT) {
           if (col >= w0 && col < w1) {
             const uint32_t o = uint32_t(col - w0);
             const uint32_t bit = 1u << (o & 31);
@@ -158,169 +236,284 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     for (int64_t i = tid; i < nw; i += kThreads) local += __popc(bm[i]);
     total += group_sum<kThreads, int64_t>(local, scan_tmp, 0);
   }
-  if (tid == 0) A.rowc[g] = int32_t(total);
+  if (tid == 0) A.rowc[rr.g] = int32_t(total);
 }
 
 // ---------------------------------------------------------------- numeric
 
-template <int G, int TMAX, typename PT, typename VT>
-__device__ void num_hash_rows(const ProdDev<PT, VT> *prods,
-                              const PhaseArgs &A, int64_t first, int64_t last,
-                              unsigned char *smem, int64_t *scan_tmp) {
-  constexpr int NG = kThreads / G;
-  constexpr int SLICE = TMAX * 12;  // FP64 value + int32 key per slot
-  constexpr int RPI = cls_rows_per_item(
-      G == 1024 ? CLS_G1024 : G == 256 ? CLS_G256 : G == 128 ? CLS_G128 : CLS_G32);
-  static_assert(NG * SLICE <= kDynSmem, "numeric table exceeds shared memory");
-  static_assert(TMAX / 2 <= 8 * G, "compaction keeps 8 first-half slots per thread");
-  const int gid = threadIdx.x / G, lane = threadIdx.x % G;
-  unsigned char *slice = smem + gid * SLICE;
-  VT *vals = (VT *)slice;
-  int *keys = (int *)(slice + TMAX * 8);
-  int64_t *tmp = scan_tmp + gid * 33;
-  for (int64_t idx = first + gid; idx < last && idx < first + RPI; idx += NG) {
-    const uint64_t e = A.list[idx];
-    const int p = int(e >> 40);
-    const int64_t r = int64_t(e & ((uint64_t(1) << 40) - 1));
-    const int64_t g = A.base[p] + r;
-    const ProdDev<PT, VT> &P = prods[p];
-    const int64_t c = A.rowc[g];
-    const int64_t off = A.cp[g] - A.cp[A.base[p]];
-    uint32_t T = pow2_at_least(2 * c, 32);
-    if (T > TMAX) T = TMAX;
-    const int logT = ilog2_pow2(T);
-    const uint32_t mask = T - 1;
-    for (uint32_t s = lane; s < T; s += G) {
-      keys[s] = -1;
-      vals[s] = VT(0);
-    }
-    group_sync<G>(gid);
-    const int64_t a0 = P.Ap[r], a1 = P.Ap[r + 1];
-    const int S = subgroup_width(A.rowf[g], a1 - a0, G);
-    for_products<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, S,
-                                  lane, [&](int32_t col, VT v) {
-                                    const uint32_t h =
-                                        num_insert(keys, col, logT, mask, A.err);
-                                    atomicAdd(vals + h, v);
-                                  });
-    group_sync<G>(gid);
-    // In-place compaction into [0, c): the targets lie in the first half of
-    // the table (c <= T/2), so only first-half slots are read into registers
-    // before the group barrier inside the scan; second-half slots are never
-    // overwritten and are read after it.
-    const uint32_t H = T >> 1;
-    int rk[8];
-    VT rv[8];
-    int64_t mine = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint32_t s = lane + i * G;
-      rk[i] = -1;
-      rv[i] = VT(0);
-      if (s < H) {
-        rk[i] = keys[s];
-        rv[i] = vals[s];
-      }
-      mine += rk[i] != -1;
-    }
-    for (uint32_t s = H + lane; s < T; s += G) mine += keys[s] != -1;
-    int64_t tot;
-    int64_t pos = group_excl_scan<G, int64_t>(mine, tmp, gid, &tot);
-    group_sync<G>(gid);
-    if (lane == 0 && tot != c) set_error(A.err, 103);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      if (rk[i] != -1) {
-        keys[pos] = rk[i];
-        vals[pos] = rv[i];
-        ++pos;
-      }
-    }
-    for (uint32_t s = H + lane; s < T; s += G) {
-      const int k = keys[s];
-      if (k != -1) {
-        const VT v = vals[s];
-        keys[pos] = k;
-        vals[pos] = v;
-        ++pos;
-      }
-    }
-    group_sync<G>(gid);
-    for (uint32_t s = uint32_t(c) + lane; s < H; s += G) keys[s] = INT32_MAX;
-    group_sync<G>(gid);
-    // Bitonic sort of the H = pow2 >= c compacted pairs by column.
-    for (uint32_t k = 2; k <= H; k <<= 1) {
-      for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-        for (uint32_t t = lane; t < (H >> 1); t += G) {
-          const uint32_t i = 2 * t - (t & (j - 1));
-          const uint32_t l = i + j;
-          const bool up = (i & k) == 0;
-          const int ki = keys[i], kl = keys[l];
-          if ((ki > kl) == up) {
-            keys[i] = kl;
-            keys[l] = ki;
-            const VT vi = vals[i];
-            vals[i] = vals[l];
-            vals[l] = vi;
-          }
+// Bitonic sort of P (pow2) pairs by key, in place.
+template <int G, typename VT>
+__device__ __forceinline__ void bitonic_pairs(int *keys, VT *vals, uint32_t P,
+                                              int gid, int lane) {
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t t = lane; t < (P >> 1); t += G) {
+        const uint32_t i = 2 * t - (t & (j - 1));
+        const uint32_t l = i + j;
+        const bool up = (i & k) == 0;
+        const int ki = keys[i], kl = keys[l];
+        if ((ki > kl) == up) {
+          keys[i] = kl;
+          keys[l] = ki;
+          const VT vi = vals[i];
+          vals[i] = vals[l];
+          vals[l] = vi;
         }
-        group_sync<G>(gid);
       }
+      group_sync<G>(gid);
     }
-    int32_t *__restrict__ Cj = P.Cj + off;
-    VT *__restrict__ Cx = P.Cx + off;
-    for (int64_t s = lane; s < c; s += G) {
-      Cj[s] = keys[s];
-      Cx[s] = vals[s];
-    }
-    group_sync<G>(gid);
   }
 }
 
-// DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry j
+// Stable LSD radix sort of n <= 8*G (key, value) pairs with 5-bit digits.
+// Element e sits at item e / G of thread e % G; within a warp, equal digits
+// are ranked with __match_any_sync.  cnt holds 32 digits x 8 items x G/32
+// warps uint16 counters laid out (digit, item, warp), so one exclusive scan
+// over cnt yields every element's output base in stable order.  (ka, va) and
+// (kb, vb) alternate as source and destination; returns 1 when the sorted
+// pairs end in (kb, vb).
+template <int G, typename VT>
+__device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
+                           uint16_t *cnt, int64_t *tmp, int gid, int lane) {
+  constexpr int NW = G / 32, ITEMS = 8, RB = 5, RAD = 1 << RB;
+  constexpr int E = RAD * ITEMS * NW, PER = E / G;
+  static_assert(PER * G == E, "counter layout");
+  const int w = lane >> 5;
+  const unsigned below = (1u << (lane & 31)) - 1u;
+  int src = 0;
+  for (int shift = 0; shift < bits; shift += RB) {
+    const int *ks = src ? kb : ka;
+    const VT *vs = src ? vb : va;
+    int *kd = src ? ka : kb;
+    VT *vd = src ? va : vb;
+    for (int i = lane; i < E; i += G) cnt[i] = 0;
+    group_sync<G>(gid);
+    int dig[ITEMS], rk[ITEMS];
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+      const int e = it * G + lane;
+      const int d = e < n ? ((ks[e] >> shift) & (RAD - 1)) : RAD;
+      const unsigned m = __match_any_sync(0xffffffffu, d);
+      rk[it] = __popc(m & below);
+      dig[it] = d;
+      if (d < RAD && rk[it] == 0) cnt[(d * ITEMS + it) * NW + w] = uint16_t(__popc(m));
+    }
+    group_sync<G>(gid);
+    int s = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) s += cnt[lane * PER + j];
+    int64_t tot;
+    int run = int(group_excl_scan<G, int64_t>(int64_t(s), tmp, gid, &tot));
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int v = cnt[lane * PER + j];
+      cnt[lane * PER + j] = uint16_t(run);
+      run += v;
+    }
+    group_sync<G>(gid);
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+      const int e = it * G + lane;
+      if (e < n) {
+        const int pos = int(cnt[(dig[it] * ITEMS + it) * NW + w]) + rk[it];
+        kd[pos] = ks[e];
+        vd[pos] = vs[e];
+      }
+    }
+    group_sync<G>(gid);
+    src ^= 1;
+  }
+  return src;
+}
+
+template <int G, int TMAX, typename PT, typename VT>
+__device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                             int64_t idx, unsigned char *slice, const GroupMem &gm,
+                             int gid, int lane) {
+  int64_t *tmp = gm.tmp;
+  int *itmp = gm.itmp;
+  uint16_t *cnt = gm.cnt;
+  static_assert(TMAX / 2 <= 8 * G, "compaction keeps 8 first-half slots per thread");
+  VT *vals = (VT *)slice;
+  int *keys = (int *)(slice + TMAX * 8);
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
+  const int64_t c = A.rowc[rr.g];
+  const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
+  uint32_t T = pow2_at_least(2 * c, 32);
+  if (T > TMAX) T = TMAX;
+  const int logT = ilog2_pow2(T);
+  const uint32_t mask = T - 1;
+  for (uint32_t s = lane; s < T; s += G) {
+    keys[s] = -1;
+    vals[s] = VT(0);
+  }
+  group_sync<G>(gid);
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int S = subgroup_width(A.rowf[rr.g], a1 - a0, G);
+  for_products_balanced<G, true, PT, VT>(
+      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl,
+      gm.cap, [&](int32_t col, VT v) {
+        const uint32_t h = num_insert(keys, col, logT, mask, A.err);
+        atomicAdd(vals + h, v);
+      });
+  group_sync<G>(gid);
+  // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
+  // so first-half slots are held in registers across the group barrier inside
+  // group_minmax; second-half slots are never overwritten.
+  const uint32_t H = T >> 1;
+  int rk[8];
+  VT rv[8];
+  int mine = 0, mn = INT32_MAX, mx = -1;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const uint32_t s = lane + i * G;
+    rk[i] = -1;
+    rv[i] = VT(0);
+    if (s < H) {
+      rk[i] = keys[s];
+      rv[i] = vals[s];
+    }
+    if (rk[i] != -1) {
+      ++mine;
+      mn = min(mn, rk[i]);
+      mx = max(mx, rk[i]);
+    }
+  }
+  for (uint32_t s = H + lane; s < T; s += G) {
+    const int k = keys[s];
+    if (k != -1) {
+      ++mine;
+      mn = min(mn, k);
+      mx = max(mx, k);
+    }
+  }
+  group_minmax<G>(mn, mx, itmp, gid);
+  int64_t tot;
+  int64_t pos = group_excl_scan<G, int64_t>(int64_t(mine), tmp, gid, &tot);
+  group_sync<G>(gid);
+  if (lane == 0 && tot != c) set_error(A.err, 103);
+  const bool radix = c > kBitonicMax;
+  const int bias = radix ? mn : 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (rk[i] != -1) {
+      keys[pos] = rk[i] - bias;
+      vals[pos] = rv[i];
+      ++pos;
+    }
+  }
+  for (uint32_t s = H + lane; s < T; s += G) {
+    const int k = keys[s];
+    if (k != -1) {
+      const VT v = vals[s];
+      keys[pos] = k - bias;
+      vals[pos] = v;
+      ++pos;
+    }
+  }
+  group_sync<G>(gid);
+  int src = 0;
+  if (!radix) {
+    const uint32_t Pw = pow2_at_least(c, 2);
+    for (uint32_t s = uint32_t(c) + lane; s < Pw; s += G) keys[s] = INT32_MAX;
+    group_sync<G>(gid);
+    bitonic_pairs<G, VT>(keys, vals, Pw, gid, lane);
+  } else {
+    const int bits = 32 - __clz(mx - mn);
+    src = radix_pairs<G, VT>(keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid, lane);
+  }
+  const int *ko = src ? keys + H : keys;
+  const VT *vo = src ? vals + H : vals;
+  int32_t *__restrict__ Cj = P.Cj + off;
+  VT *__restrict__ Cx = P.Cx + off;
+  for (int64_t s = lane; s < c; s += G) {
+    Cj[s] = ko[s] + bias;
+    Cx[s] = vo[s];
+  }
+  group_sync<G>(gid);
+}
+
+// DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry
 // keeps a cursor into its (sorted) B row, so every B entry is read once; the
-// window's accumulator is dense FP64 plus a presence bitmap, and the window
-// is emitted in column order.  With unsorted B every window rescans the rows.
+// window's accumulator is dense FP64 plus a presence bitmap, and the window is
+// emitted in column order.  B rows longer than a sub-group's fair share are
+// listed once per row; in each window their segment end is found by binary
+// search and the whole CTA walks the segment.  With unsorted B every window
+// rescans the rows (no cursors, no list).
 template <typename PT, typename VT>
 __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
-                              int64_t idx, unsigned char *smem,
-                              int64_t *scan_tmp) {
+                              int64_t idx, unsigned char *smem, const GroupMem &gm) {
+  constexpr int kLongMark = INT32_MIN;
   const int tid = threadIdx.x, lane = tid & 31;
+  int64_t *scan_tmp = gm.tmp;
   VT *acc = (VT *)smem;
   uint32_t *bm = (uint32_t *)(smem + kDenseW * 8);
   int32_t *cur_s = (int32_t *)(smem + kDenseW * 8 + kDenseW / 8);
-  const uint64_t e = A.list[idx];
-  const int p = int(e >> 40);
-  const int64_t r = int64_t(e & ((uint64_t(1) << 40) - 1));
-  const int64_t g = A.base[p] + r;
-  const ProdDev<PT, VT> &P = prods[p];
+  int32_t *lcur = cur_s + kDenseCurSmem;  // cursor of listed entry i
+  int32_t *lend = lcur + 1024;            // its segment end in this window
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t n = P.n;
-  const int64_t a0 = P.Ap[r], a1 = P.Ap[r + 1], na = a1 - a0;
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1], na = a1 - a0;
+  const int64_t f = A.rowf[rr.g];
   int32_t *cur = na <= kDenseCurSmem ? cur_s : A.curbuf + blockIdx.x * A.cur_stride;
   const bool sorted = P.b_sorted != 0;
-  for (int64_t j = tid; j < na; j += kThreads) cur[j] = 0;
-  for (int i = tid; i < kDenseW; i += kThreads) acc[i] = VT(0);
-  for (int i = tid; i < kDenseW / 32; i += kThreads) bm[i] = 0u;
-  __syncthreads();
-  int64_t out = A.cp[g] - A.cp[A.base[p]];
-  const int S = subgroup_width(A.rowf[g], na, 32);
-  const int sl = lane % S;
-  const int subid = tid / S, nsub = kThreads / S;
-  const unsigned submask =
-      S == 32 ? 0xffffffffu : (((1u << S) - 1u) << ((lane / S) * S));
   const int32_t *__restrict__ Aj = P.Aj;
   const VT *__restrict__ Ax = P.Ax;
   const PT *__restrict__ Bp = P.Bp;
   const int32_t *__restrict__ Bj = P.Bj;
   const VT *__restrict__ Bx = P.Bx;
+  const int S = subgroup_width(f, na, 32);
+  const int sl = lane % S;
+  const int subid = tid / S, nsub = kThreads / S;
+  const unsigned submask =
+      S == 32 ? 0xffffffffu : (((1u << S) - 1u) << ((lane / S) * S));
+  const int64_t thr = max(int64_t(4 * S), f / nsub);
+  if (tid == 0) *gm.nl = 0;
+  for (int i = tid; i < kDenseW; i += kThreads) acc[i] = VT(0);
+  for (int i = tid; i < kDenseW / 32; i += kThreads) bm[i] = 0u;
+  __syncthreads();
+  // classify: listed (long) entries get the cursor mark
+  for (int64_t j = subid; j < na; j += nsub) {
+    int mark = 0;
+    if (sorted && sl == 0) {
+      const int64_t k = __ldg(Aj + a0 + j);
+      if (__ldg(Bp + k + 1) - __ldg(Bp + k) > thr) {
+        const int slot = atomicAdd(gm.nl, 1);
+        if (slot < gm.cap) {
+          gm.lst[slot] = int(j);
+          lcur[slot] = 0;
+          mark = kLongMark;
+        }
+      }
+    }
+    if (sl == 0) cur[j] = mark;
+  }
+  __syncthreads();
+  const int nl = min(*gm.nl, gm.cap);
+  int64_t out = A.cp[rr.g] - A.cp[A.base[rr.p]];
   for (int64_t w0 = 0; w0 < n; w0 += kDenseW) {
     const int64_t w1 = (w0 + kDenseW < n) ? w0 + kDenseW : n;
+    // segment ends of the listed entries in this window
+    for (int i = tid; i < nl; i += kThreads) {
+      const int64_t k = __ldg(Aj + a0 + gm.lst[i]);
+      int64_t lo = __ldg(Bp + k) + lcur[i], hi = __ldg(Bp + k + 1);
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(Bj + mid) < w1) lo = mid + 1; else hi = mid;
+      }
+      lend[i] = int32_t(lo - __ldg(Bp + k));
+    }
+    // short entries: sub-groups with cursors
     for (int64_t j = subid; j < na; j += nsub) {
       const int64_t k = __ldg(Aj + a0 + j);
       const VT a = __ldg(Ax + a0 + j);
       const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
       if (sorted) {
-        int64_t q = b0 + cur[j];
+        const int32_t c0 = cur[j];
+        if (c0 == kLongMark) continue;
+        int64_t q = b0 + c0;
         while (q < b1) {
           const int64_t qq = q + sl;
           const bool valid = qq < b1;
@@ -350,7 +543,23 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
         }
       }
     }
+    __syncthreads();  // lend[] ready
+    // long entries: the whole CTA walks [lcur, lend)
+    for (int i = 0; i < nl; ++i) {
+      const int64_t p = a0 + gm.lst[i];
+      const int64_t k = __ldg(Aj + p);
+      const VT a = __ldg(Ax + p);
+      const int64_t b0 = __ldg(Bp + k);
+      const int64_t e = b0 + lend[i];
+      for (int64_t q = b0 + lcur[i] + tid; q < e; q += kThreads) {
+        const uint32_t o = uint32_t(__ldg(Bj + q) - w0);
+        atomicAdd(acc + o, a * __ldg(Bx + q));
+        const uint32_t bit = 1u << (o & 31);
+        if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
+      }
+    }
     __syncthreads();
+    for (int i = tid; i < nl; i += kThreads) lcur[i] = lend[i];
     uint32_t word = tid < kDenseW / 32 ? bm[tid] : 0u;
     int64_t tot;
     int64_t pos = group_excl_scan<kThreads, int64_t>(int64_t(__popc(word)),
@@ -372,49 +581,116 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
 }
 
+// ---------------------------------------------------------------- the kernel
+
+struct PhaseShared {
+  int64_t scan[16 * 33];      // group scan scratch: 256-groups 0-3, 128-groups 4-11
+  int itmp[12 * 18];          // group min/max scratch, same slots
+  unsigned long long slot[16];  // fetched row index per group; [15] = CTA
+  int lst[1024];              // deferred long B rows: CTA 1024, 256-group g at 256g,
+                              // 128-group g at 128g, warp w at 32w
+  int nl[48];                 // list counts: 256-groups 0-3, 128-groups 4-11,
+                              // warps 12-43, CTA 47
+  int64_t off[NCLS], cnt[NCLS];
+};
+
+// Group-level rows of class `cls`: the group leader fetches one row index at a
+// time; the group exits when the class runs out.
+template <int G, bool NUM, typename PT, typename VT>
+__device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                           int cls, unsigned char *smem, PhaseShared &sh) {
+  constexpr int SLICE = NUM ? kTableSmem / (kThreads / G) : (kTableSmem * 2 / 3) / (kThreads / G);
+  constexpr int TMAXS = G == 256 ? kSymT256 : G == 128 ? kSymT128 : kSymT32;
+  constexpr int TMAXN = G == 256 ? kNumT256 : G == 128 ? kNumT128 : kNumT32;
+  static_assert(!NUM || TMAXN * 12 <= SLICE, "numeric slice");
+  static_assert(NUM || TMAXS * 4 <= SLICE, "symbolic slice");
+  const int gid = threadIdx.x / G, lane = threadIdx.x % G;
+  const int slot = G == 256 ? gid : G == 128 ? 4 + gid : 0;
+  unsigned char *slice = smem + gid * SLICE;
+  GroupMem gm;
+  gm.cnt = (uint16_t *)(smem + kTableSmem) + gid * (32 * 8 * (G / 32));
+  gm.tmp = sh.scan + slot * 33;
+  gm.itmp = sh.itmp + slot * 18;
+  gm.lst = sh.lst + gid * G;
+  gm.nl = sh.nl + (G == 32 ? 12 + gid : slot);
+  gm.cap = G;
+  const int64_t base = sh.off[cls], count = sh.cnt[cls];
+  while (true) {
+    int64_t i;
+    if constexpr (G == 32) {
+      unsigned long long v = 0;
+      if (lane == 0) v = atomicAdd(&A.S->next[cls], 1ull);
+      i = (int64_t)__shfl_sync(0xffffffffu, v, 0);
+    } else {
+      if (lane == 0) sh.slot[slot] = atomicAdd(&A.S->next[cls], 1ull);
+      group_sync<G>(gid);
+      i = (int64_t)sh.slot[slot];
+      group_sync<G>(gid);
+    }
+    if (i >= count) break;
+    const long long t0 = clock64();
+    if constexpr (NUM)
+      num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+    else
+      sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+    prof_add(A, cls, t0, lane == 0);
+  }
+}
+
 template <typename PT, typename VT, bool NUM>
 __global__ void __launch_bounds__(kThreads, 1)
     k_phase(const ProdDev<PT, VT> *prods, PhaseArgs A) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int64_t s_items[NCLS + 1], s_off[NCLS], s_cnt[NCLS];
-  __shared__ unsigned long long s_item;
-  __shared__ int64_t s_scan[16 * 33];
+  __shared__ PhaseShared sh;
+  __shared__ int64_t s_items[kCtaClasses + 1];
   const int tid = threadIdx.x;
-  if (tid <= NCLS) s_items[tid] = A.S->items[tid];
   if (tid < NCLS) {
-    s_off[tid] = A.S->off[tid];
-    s_cnt[tid] = A.S->cnt[tid];
+    sh.off[tid] = A.S->off[tid];
+    sh.cnt[tid] = A.S->cnt[tid];
+  }
+  if (tid == 0) {
+    int64_t it = 0;
+    for (int c = 0; c < kCtaClasses; ++c) {
+      s_items[c] = it;
+      it += A.S->cnt[c];
+    }
+    s_items[kCtaClasses] = it;
   }
   __syncthreads();
-  const int64_t total = s_items[NCLS];
+  GroupMem gm;
+  gm.cnt = (uint16_t *)(smem + kTableSmem);
+  gm.tmp = sh.scan;
+  gm.itmp = sh.itmp;
+  gm.lst = sh.lst;
+  gm.nl = sh.nl + 47;
+  gm.cap = 1024;
+  // stage 1: CTA-level rows, heaviest class first
   while (true) {
-    if (tid == 0) s_item = atomicAdd(&A.S->work, 1ull);
+    if (tid == 0) sh.slot[15] = atomicAdd(&A.S->work, 1ull);
     __syncthreads();
-    const int64_t item = (int64_t)s_item;
-    if (item >= total) break;
+    const int64_t item = (int64_t)sh.slot[15];
+    __syncthreads();
+    if (item >= s_items[kCtaClasses]) break;
     int c = 0;
     while (item >= s_items[c + 1]) ++c;
-    const int64_t first = s_off[c] + (item - s_items[c]) * cls_rows_per_item(c);
-    const int64_t last = s_off[c] + s_cnt[c];
-    if constexpr (!NUM) {
-      switch (c) {
-        case CLS_DENSE: sym_dense_row<PT, VT>(prods, A, first, smem, s_scan); break;
-        case CLS_G1024: sym_hash_rows<1024, kSymT1024, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        case CLS_G256: sym_hash_rows<256, kSymT256, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        case CLS_G128: sym_hash_rows<128, kSymT128, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        default: sym_hash_rows<32, kSymT32, PT, VT>(prods, A, first, last, smem, s_scan); break;
-      }
+    const int64_t idx = sh.off[c] + (item - s_items[c]);
+    const long long t0 = clock64();
+    if (cls_dense(c)) {
+      if constexpr (NUM) num_dense_row<PT, VT>(prods, A, idx, smem, gm);
+      else sym_dense_row<PT, VT>(prods, A, idx, smem, gm);
     } else {
-      switch (c) {
-        case CLS_DENSE: num_dense_row<PT, VT>(prods, A, first, smem, s_scan); break;
-        case CLS_G1024: num_hash_rows<1024, kNumT1024, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        case CLS_G256: num_hash_rows<256, kNumT256, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        case CLS_G128: num_hash_rows<128, kNumT128, PT, VT>(prods, A, first, last, smem, s_scan); break;
-        default: num_hash_rows<32, kNumT32, PT, VT>(prods, A, first, last, smem, s_scan); break;
-      }
+      if constexpr (NUM)
+        num_hash_row<kThreads, kNumT1024, PT, VT>(prods, A, idx, smem, gm, 0, tid);
+      else
+        sym_hash_row<kThreads, kSymT1024, PT, VT>(prods, A, idx, (int *)smem, gm, 0, tid);
     }
+    prof_add(A, c, t0, tid == 0);
     __syncthreads();
   }
+  // stage 2: nested groups, no CTA-wide barrier from here on
+  group_rows<256, NUM, PT, VT>(prods, A, CLS_G256, smem, sh);
+  group_rows<128, NUM, PT, VT>(prods, A, CLS_G128, smem, sh);
+  group_rows<32, NUM, PT, VT>(prods, A, CLS_G32, smem, sh);
 }
 
 }  // namespace tspg
