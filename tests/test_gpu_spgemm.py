@@ -163,3 +163,14 @@ def test_sorted_flag_skips_check(ctx):
     A = workloads.uniform_rows(2048, 16, True, seed=7)
     dA = A.to_device()
     check_product(ops.spgemm(ctx, dA, dA, flags=TSPG_F_B_SORTED), A, A)
+
+
+def test_dense_rows_wide_b_windowed(ctx):
+    # ncols above the whole-row bitmap limit: DENSE rows take the windowed
+    # sweep (sorted B with cursors, then unsorted B with rescans)
+    n = 1_300_000
+    B = random_csr(3000, n, per_row=40, seed=21)
+    A = random_csr(6, 3000, per_row=600, seed=22)
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+    Bu = random_csr(3000, n, per_row=40, seed=23, sort=False)
+    check_product(ops.spgemm(ctx, A.to_device(), Bu.to_device()), A, Bu)

@@ -64,6 +64,8 @@ constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory
 constexpr int64_t kDenseBits = int64_t(kTableSmem) * 8;  // symbolic bitmap
 constexpr int kBitonicMax = 64;          // rows up to this size sort bitonic
+// whole-row DENSE numeric form: bitmap (4 B) + uint16 rank offset per 32 columns
+constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 6) * 32;
 
 __host__ __device__ inline int dense_sub(int64_t f) {
   return f >= (int64_t(1) << 20) ? CLS_DENSE0 : f >= (int64_t(1) << 17) ? CLS_DENSE1 : CLS_DENSE2;

@@ -434,6 +434,72 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   group_sync<G>(gid);
 }
 
+// DENSE numeric row, whole-row form (ncols <= kRankMaxCols).  Pass 1 sets the
+// row's column bitmap; a CTA scan of the bitmap gives every word's rank base
+// (per-thread chunk base + uint16 offset inside the chunk) and writes the
+// sorted column indices and zeroed values of the row's output; pass 2 adds
+// every product into its output slot, found as base + popc of the bits below,
+// with a global FP64 reduction (the row's output segment is L2-resident while
+// the CTA works on it).  No windows, no sort.
+template <typename PT, typename VT>
+__device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                                   int64_t idx, unsigned char *smem, const GroupMem &gm,
+                                   int *tbase) {
+  const int tid = threadIdx.x;
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
+  const int64_t n = P.n;
+  const int nw = int((n + 31) >> 5);
+  uint32_t *bm = (uint32_t *)smem;
+  uint16_t *wp = (uint16_t *)(smem + size_t(nw) * 4);
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int64_t f = A.rowf[rr.g];
+  const int S = subgroup_width(f, a1 - a0, 32);
+  for (int i = tid; i < nw; i += kThreads) bm[i] = 0u;
+  __syncthreads();
+  for_products_balanced<kThreads, false, PT, VT>(
+      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, tid, 0, gm.lst, gm.nl, gm.cap,
+      [&](int32_t col, VT) {
+        const uint32_t bit = 1u << (col & 31);
+        if (!(((volatile uint32_t *)bm)[col >> 5] & bit)) atomicOr(bm + (col >> 5), bit);
+      });
+  __syncthreads();
+  // chunk of 2^lc consecutive words per thread
+  int lc = 0;
+  while ((kThreads << lc) < nw) ++lc;
+  const int w0 = tid << lc, w1 = min(nw, (tid + 1) << lc);
+  int cnt = 0;
+  for (int w = w0; w < w1; ++w) cnt += __popc(bm[w]);
+  int64_t tot;
+  const int base = int(group_excl_scan<kThreads, int64_t>(int64_t(cnt), gm.tmp, 0, &tot));
+  tbase[tid] = base;
+  const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
+  int32_t *__restrict__ Cj = P.Cj + off;
+  VT *__restrict__ Cx = P.Cx + off;
+  int run = 0;
+  for (int w = w0; w < w1; ++w) {
+    uint32_t word = bm[w];
+    wp[w] = uint16_t(run);
+    while (word) {
+      const int b = __ffs(word) - 1;
+      word &= word - 1;
+      Cj[base + run] = int32_t(w * 32 + b);
+      Cx[base + run] = VT(0);
+      ++run;
+    }
+  }
+  if (tid == 0 && tot != A.rowc[rr.g]) set_error(A.err, 104);
+  __threadfence();
+  __syncthreads();
+  for_products_balanced<kThreads, true, PT, VT>(
+      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, tid, 0, gm.lst, gm.nl, gm.cap,
+      [&](int32_t col, VT v) {
+        const int w = col >> 5;
+        const int rank = tbase[w >> lc] + int(wp[w]) + __popc(bm[w] & ((1u << (col & 31)) - 1u));
+        atomicAdd(Cx + rank, v);
+      });
+}
+
 // DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry
 // keeps a cursor into its (sorted) B row, so every B entry is read once; the
 // window's accumulator is dense FP64 plus a presence bitmap, and the window is
@@ -464,12 +530,14 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const PT *__restrict__ Bp = P.Bp;
   const int32_t *__restrict__ Bj = P.Bj;
   const VT *__restrict__ Bx = P.Bx;
-  const int S = subgroup_width(f, na, 32);
+  // sub-group width from the per-window segment length of an average B row
+  const int64_t nwin = (n + kDenseW - 1) / kDenseW;
+  const int S = subgroup_width(f / nwin, na, 32);
   const int sl = lane % S;
   const int subid = tid / S, nsub = kThreads / S;
   const unsigned submask =
       S == 32 ? 0xffffffffu : (((1u << S) - 1u) << ((lane / S) * S));
-  const int64_t thr = max(int64_t(4 * S), f / nsub);
+  const int64_t thr = max(int64_t(4 * S) * nwin, f / nsub);
   if (tid == 0) *gm.nl = 0;
   for (int i = tid; i < kDenseW; i += kThreads) acc[i] = VT(0);
   for (int i = tid; i < kDenseW / 32; i += kThreads) bm[i] = 0u;
@@ -643,6 +711,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ PhaseShared sh;
   __shared__ int64_t s_items[kCtaClasses + 1];
+  __shared__ int s_tbase[NUM ? kThreads : 1];
   const int tid = threadIdx.x;
   if (tid < NCLS) {
     sh.off[tid] = A.S->off[tid];
@@ -676,8 +745,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int64_t idx = sh.off[c] + (item - s_items[c]);
     const long long t0 = clock64();
     if (cls_dense(c)) {
-      if constexpr (NUM) num_dense_row<PT, VT>(prods, A, idx, smem, gm);
-      else sym_dense_row<PT, VT>(prods, A, idx, smem, gm);
+      if constexpr (NUM) {
+        if (prods[decode_row(A, idx).p].n <= kRankMaxCols)
+          num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm, s_tbase);
+        else
+          num_dense_row<PT, VT>(prods, A, idx, smem, gm);
+      } else {
+        sym_dense_row<PT, VT>(prods, A, idx, smem, gm);
+      }
     } else {
       if constexpr (NUM)
         num_hash_row<kThreads, kNumT1024, PT, VT>(prods, A, idx, smem, gm, 0, tid);
