@@ -12,23 +12,26 @@
 //
 // Row classes (the same five for both phases, heaviest first so that the
 // persistent grid starts on the long rows):
-//   DENSE  one 1024-thread CTA per row, dense shared-memory window:
-//          symbolic = bitmap of up to 1.5M columns, numeric = FP64 window of
-//          16384 columns swept left to right with per-A-entry cursors into
-//          the sorted B rows; output is sorted by construction.
+//   DENSE  (three sub-classes by product count, heaviest first) one CTA per
+//          row.  Symbolic: a bitmap of the whole column range in shared
+//          memory.  Numeric: the same bitmap, then a CTA scan that writes the
+//          sorted columns and keeps a rank base per 32 columns; every product
+//          is then added into its output slot with a global FP64 reduction
+//          (rows wider than the shared-memory bitmap use an FP64 window of
+//          16384 columns swept with per-A-entry cursors instead).
 //   G1024  one CTA per row, open-addressing hash in shared memory.
-//   G256   4 rows per CTA (256-thread groups, named barriers).
-//   G128   8 rows per CTA.
-//   G32    one warp per row, 2 rows per warp per work item.
+//   G256   256-thread groups, named barriers.
+//   G128   128-thread groups.
+//   G32    one warp per row.
 // Hash rows are sorted after accumulation by an in-place compaction into the
-// first half of the table and a bitonic sort of the compacted pairs.
+// first half of the table and a stable LSD radix sort (bitonic below 65).
 #pragma once
 
 #include "internal.cuh"
 
 namespace tspg {
 
-constexpr int kThreads = 1024;
+constexpr int kThreads = 512;   // persistent CTA: 16 warps x 128 registers
 constexpr int kTableSmem = 196608;              // hash tables / dense window
 constexpr int kCountSmem = 16384;               // radix-sort digit counters
 constexpr int kDynSmem = kTableSmem + kCountSmem;  // one CTA per SM
@@ -62,7 +65,7 @@ constexpr int kNumT32 = 512, kNumT128 = 2048, kNumT256 = 4096,
               kNumT1024 = 16384;
 constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory
-constexpr int64_t kDenseBits = int64_t(kTableSmem) * 8;  // symbolic bitmap
+constexpr int64_t kDenseBits = int64_t(kTableSmem + kCountSmem) * 8;  // whole-row bitmap
 constexpr int kBitonicMax = 64;          // rows up to this size sort bitonic
 // whole-row DENSE numeric form: bitmap (4 B) + uint16 rank offset per 32 columns
 constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 6) * 32;

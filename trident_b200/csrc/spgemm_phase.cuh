@@ -1,10 +1,10 @@
 // spgemm_phase.cuh — the persistent symbolic / numeric kernels.
 //
-// One 1024-thread CTA per SM (208 KiB of dynamic shared memory).  Work is
-// taken in two stages:
+// One 512-thread CTA per SM (208 KiB of dynamic shared memory, 128 registers
+// per thread).  Work is taken in two stages:
 //   1. CTA-level rows (DENSE0..2 heaviest first, then G1024): thread 0 takes
 //      the next row index from a device counter, the whole CTA works on it.
-//   2. When those run out, the CTA splits into four 256-thread groups that
+//   2. When those run out, the CTA splits into two 256-thread groups that
 //      take G256 rows from their own counter; a group that runs out splits
 //      into two 128-thread groups (G128 rows), which split into warps (G32
 //      rows).  Groups never wait for each other: their shared-memory slices
@@ -16,6 +16,33 @@
 #include "spgemm_kernels.cuh"
 
 namespace tspg {
+
+// Walk B entries q0, q0 + step, ... below b1 calling fn(col, a*b), with U
+// loads in flight per thread (all loads of a step are issued before the
+// updates, so the L2/HBM latency is paid once per U entries).
+template <bool NUM, typename VT, typename F>
+__device__ __forceinline__ void walk_row(const int32_t *__restrict__ Bj,
+                                         const VT *__restrict__ Bx, int64_t q0,
+                                         int64_t b1, int step, VT a, F &&fn) {
+  constexpr int U = 4;
+  for (int64_t q = q0; q < b1; q += int64_t(step) * U) {
+    int32_t c[U];
+    VT x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t qq = q + int64_t(u) * step;
+      c[u] = qq < b1 ? __ldg(Bj + qq) : -1;
+      if constexpr (NUM) x[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (c[u] >= 0) {
+        if constexpr (NUM) fn(c[u], a * x[u]);
+        else fn(c[u], VT(0));
+      }
+    }
+  }
+}
 
 // Product loop: sub-groups of S threads take A entries in turn; the S threads
 // of a sub-group stride over that entry's B row.  f(col, a*b) per product.
@@ -32,11 +59,7 @@ __device__ __forceinline__ void for_products(const int32_t *__restrict__ Aj,
     const int64_t k = __ldg(Aj + p);
     VT a = VT(0);
     if constexpr (NUM) a = __ldg(Ax + p);
-    const int64_t b1 = __ldg(Bp + k + 1);
-    for (int64_t q = __ldg(Bp + k) + sl; q < b1; q += S) {
-      if constexpr (NUM) f(__ldg(Bj + q), a * __ldg(Bx + q));
-      else f(__ldg(Bj + q), VT(0));
-    }
+    walk_row<NUM, VT>(Bj, Bx, __ldg(Bp + k) + sl, __ldg(Bp + k + 1), S, a, f);
   }
 }
 
@@ -72,10 +95,7 @@ __device__ __forceinline__ void for_products_balanced(
     }
     VT a = VT(0);
     if constexpr (NUM) a = __ldg(Ax + p);
-    for (int64_t q = b0 + sl; q < b1; q += S) {
-      if constexpr (NUM) fn(__ldg(Bj + q), a * __ldg(Bx + q));
-      else fn(__ldg(Bj + q), VT(0));
-    }
+    walk_row<NUM, VT>(Bj, Bx, b0 + sl, b1, S, a, fn);
   }
   group_sync<G>(gid);
   const int n = min(*nl, cap);
@@ -84,11 +104,7 @@ __device__ __forceinline__ void for_products_balanced(
     const int64_t k = __ldg(Aj + p);
     VT a = VT(0);
     if constexpr (NUM) a = __ldg(Ax + p);
-    const int64_t b1 = __ldg(Bp + k + 1);
-    for (int64_t q = __ldg(Bp + k) + lane; q < b1; q += G) {
-      if constexpr (NUM) fn(__ldg(Bj + q), a * __ldg(Bx + q));
-      else fn(__ldg(Bj + q), VT(0));
-    }
+    walk_row<NUM, VT>(Bj, Bx, __ldg(Bp + k) + lane, __ldg(Bp + k + 1), G, a, fn);
   }
 }
 
@@ -265,17 +281,17 @@ __device__ __forceinline__ void bitonic_pairs(int *keys, VT *vals, uint32_t P,
   }
 }
 
-// Stable LSD radix sort of n <= 8*G (key, value) pairs with 5-bit digits.
+// Stable LSD radix sort of n <= ITEMS*G (key, value) pairs with 5-bit digits.
 // Element e sits at item e / G of thread e % G; within a warp, equal digits
-// are ranked with __match_any_sync.  cnt holds 32 digits x 8 items x G/32
+// are ranked with __match_any_sync.  cnt holds 32 digits x ITEMS x G/32
 // warps uint16 counters laid out (digit, item, warp), so one exclusive scan
 // over cnt yields every element's output base in stable order.  (ka, va) and
 // (kb, vb) alternate as source and destination; returns 1 when the sorted
 // pairs end in (kb, vb).
-template <int G, typename VT>
+template <int G, int ITEMS, typename VT>
 __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
                            uint16_t *cnt, int64_t *tmp, int gid, int lane) {
-  constexpr int NW = G / 32, ITEMS = 8, RB = 5, RAD = 1 << RB;
+  constexpr int NW = G / 32, RB = 5, RAD = 1 << RB;
   constexpr int E = RAD * ITEMS * NW, PER = E / G;
   static_assert(PER * G == E, "counter layout");
   const int w = lane >> 5;
@@ -333,7 +349,8 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   int64_t *tmp = gm.tmp;
   int *itmp = gm.itmp;
   uint16_t *cnt = gm.cnt;
-  static_assert(TMAX / 2 <= 8 * G, "compaction keeps 8 first-half slots per thread");
+  constexpr int KEEP = TMAX / (2 * G);  // first-half slots held per thread
+  static_assert(KEEP >= 1 && KEEP <= 16 && KEEP * 2 * G == TMAX, "compaction layout");
   VT *vals = (VT *)slice;
   int *keys = (int *)(slice + TMAX * 8);
   const RowRef rr = decode_row(A, idx);
@@ -362,11 +379,11 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   // so first-half slots are held in registers across the group barrier inside
   // group_minmax; second-half slots are never overwritten.
   const uint32_t H = T >> 1;
-  int rk[8];
-  VT rv[8];
+  int rk[KEEP];
+  VT rv[KEEP];
   int mine = 0, mn = INT32_MAX, mx = -1;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < KEEP; ++i) {
     const uint32_t s = lane + i * G;
     rk[i] = -1;
     rv[i] = VT(0);
@@ -396,7 +413,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const bool radix = c > kBitonicMax;
   const int bias = radix ? mn : 0;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
+  for (int i = 0; i < KEEP; ++i) {
     if (rk[i] != -1) {
       keys[pos] = rk[i] - bias;
       vals[pos] = rv[i];
@@ -421,7 +438,8 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     bitonic_pairs<G, VT>(keys, vals, Pw, gid, lane);
   } else {
     const int bits = 32 - __clz(mx - mn);
-    src = radix_pairs<G, VT>(keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid, lane);
+    src = radix_pairs<G, KEEP, VT>(keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid,
+                                   lane);
   }
   const int *ko = src ? keys + H : keys;
   const VT *vo = src ? vals + H : vals;
@@ -619,12 +637,12 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       const VT a = __ldg(Ax + p);
       const int64_t b0 = __ldg(Bp + k);
       const int64_t e = b0 + lend[i];
-      for (int64_t q = b0 + lcur[i] + tid; q < e; q += kThreads) {
-        const uint32_t o = uint32_t(__ldg(Bj + q) - w0);
-        atomicAdd(acc + o, a * __ldg(Bx + q));
+      walk_row<true, VT>(Bj, Bx, b0 + lcur[i] + tid, e, kThreads, a, [&](int32_t col, VT v) {
+        const uint32_t o = uint32_t(col - w0);
+        atomicAdd(acc + o, v);
         const uint32_t bit = 1u << (o & 31);
         if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
-      }
+      });
     }
     __syncthreads();
     for (int i = tid; i < nl; i += kThreads) lcur[i] = lend[i];
@@ -676,7 +694,7 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const int slot = G == 256 ? gid : G == 128 ? 4 + gid : 0;
   unsigned char *slice = smem + gid * SLICE;
   GroupMem gm;
-  gm.cnt = (uint16_t *)(smem + kTableSmem) + gid * (32 * 8 * (G / 32));
+  gm.cnt = (uint16_t *)(smem + kTableSmem) + gid * (32 * (TMAXN / (2 * G)) * (G / 32));
   gm.tmp = sh.scan + slot * 33;
   gm.itmp = sh.itmp + slot * 18;
   gm.lst = sh.lst + gid * G;
@@ -746,7 +764,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const long long t0 = clock64();
     if (cls_dense(c)) {
       if constexpr (NUM) {
-        if (prods[decode_row(A, idx).p].n <= kRankMaxCols)
+        const ProdDev<PT, VT> &P = prods[decode_row(A, idx).p];
+        if (P.n <= kRankMaxCols)
           num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm, s_tbase);
         else
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);
