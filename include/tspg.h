@@ -55,7 +55,8 @@ enum {
   TSPG_EOVERFLOW = 3,  /* int32 row offsets requested but nnz > INT32_MAX */
   TSPG_ETIMEOUT = 4,   /* a bounded device wait gave up */
   TSPG_ECUDA = 5,      /* a CUDA runtime call failed (see tspg_last_cuda_error) */
-  TSPG_EUNSORTED = 6   /* an operand that must have sorted rows does not */
+  TSPG_EUNSORTED = 6,  /* an operand that must have sorted rows does not */
+  TSPG_ESCRATCH = 7    /* larger than the static scratch of tspg_pack_noalloc */
 };
 
 /* Major dimension of a compressed sparse matrix (mmio::MajorDim). */
@@ -217,6 +218,24 @@ int tspg_bitmask_and(tspg_ctx *ctx, void *stream, const uint8_t *a,
 int tspg_pack(tspg_ctx *ctx, void *stream, const tspg_csr *M, int major,
               const uint8_t *mask, void *out_buf, size_t cap,
               int64_t *nnz_kept_dev, int64_t *nnz_kept_host);
+
+/* tspg_pack_noalloc — the same pack as tspg_pack for callers that cannot
+ * allocate device memory, e.g. a communication thread that packs the next
+ * tile while compute and transfers run on other streams, where the implicit
+ * device synchronisation of cudaMalloc / cudaFree would stall that overlap.
+ * No counterpart in the reference (its select_entries_cuda / select_ptrs
+ * allocate per call).  Takes no context, allocates nothing and never
+ * synchronises; the kept count is written to the device int64 *nnz_kept_dev
+ * when non-NULL.  Scratch is one static device array in the library (about
+ * 3 MiB per GPU, held until exit) sized for tiles of up to
+ * TSPG_PACK_NOALLOC_MAX_SEGMENTS segments; larger tiles return
+ * TSPG_ESCRATCH.  The first call on a device looks up that array's device
+ * address (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+#define TSPG_PACK_NOALLOC_MAX_SEGMENTS 262144
+int tspg_pack_noalloc(void *stream, const tspg_csr *M, int major,
+                      const uint8_t *mask, void *out_buf, size_t cap,
+                      int64_t *nnz_kept_dev);
 
 /* Size in bytes of a packed tile (CSX_buf_size / compute_message_size,
  * src/hns_spgemm.cu:23-26). */

@@ -12,7 +12,8 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtspg.so")
 
-TSPG_OK, TSPG_EINVAL, TSPG_ENOMEM, TSPG_EOVERFLOW, TSPG_ETIMEOUT, TSPG_ECUDA, TSPG_EUNSORTED = range(7)
+TSPG_OK, TSPG_EINVAL, TSPG_ENOMEM, TSPG_EOVERFLOW, TSPG_ETIMEOUT, TSPG_ECUDA, TSPG_EUNSORTED, TSPG_ESCRATCH = range(8)
+TSPG_PACK_NOALLOC_MAX_SEGMENTS = 262144
 TSPG_ROWS, TSPG_COLS = 0, 1
 TSPG_F_B_SORTED = 1
 
@@ -103,6 +104,7 @@ def _load() -> C.CDLL:
         "tspg_bitmask_and": (i32, [vp, vp, vp, vp, i64, vp]),
         "tspg_pack": (i32, [vp, vp, P(TspgCsr), i32, vp, vp, sz, vp, P(i64)]),
         "tspg_packed_bytes": (sz, [i64, i64, i32, i32]),
+        "tspg_pack_noalloc": (i32, [vp, P(TspgCsr), i32, vp, vp, sz, vp]),
         "tspg_unpack": (i32, [vp, i64, i64, i32, i64, i32, i32, P(TspgCsr)]),
         "tspg_host_free": (None, [P(TspgHostCsr)]),
         "tspg_gen_uniform_rows": (i32, [i64, i32, i32, C.c_uint64, P(TspgHostCsr)]),

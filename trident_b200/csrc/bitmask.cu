@@ -15,6 +15,7 @@
 // search, then advanced), writing values and indices together.  The kept
 // count never leaves the device unless the caller asks for it.
 #include "internal.cuh"
+#include "pack_kernels.cuh"
 #include "spgemm_kernels.cuh"
 
 namespace tspg {
@@ -51,66 +52,6 @@ __global__ void k_bitmask_and(const uint8_t *a, const uint8_t *b,
     done = nv << 4;
   }
   for (int64_t i = done + t; i < nbytes; i += stride) out[i] = a[i] & b[i];
-}
-
-// Masked segment lengths (select_ptrs' MaskedTransform, spacomm.cuh:539-553).
-template <typename PT>
-__global__ void k_pack_counts(const PT *ptr, int64_t len, const uint8_t *mask,
-                              int32_t *cnt) {
-  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < len) {
-    const bool keep = (mask[i >> 3] >> (i & 7)) & 1;
-    cnt[i] = keep ? int32_t(int64_t(ptr[i + 1]) - int64_t(ptr[i])) : 0;
-  }
-}
-
-constexpr int kPackItems = 8;
-
-// Copy pass.  Entry e belongs to the last segment r with ptr[r] <= e (the
-// reference's locate_segment_by_pos, spacomm.cuh:714-725); it is kept iff bit
-// r is set and goes to newp[r] + (e - ptr[r]).  The pointer region starts at
-// kept*(val+4) bytes rounded up to the pointer width (no padding for the
-// reference's int32 pointers; at most 4 bytes for int64 ones).
-template <typename PT, int VB>
-__global__ void __launch_bounds__(256)
-    k_pack_copy(const PT *ptr, int64_t len, const int32_t *idx, const void *val,
-                const uint8_t *mask, const int64_t *newp, char *out,
-                int64_t *kept_dev) {
-  using V = typename std::conditional<VB == 8, unsigned long long, unsigned>::type;
-  const int64_t kept = newp[len];
-  const int64_t nnz = ptr[len];
-  V *oval = (V *)out;
-  int32_t *oidx = (int32_t *)(out + kept * VB);
-  const V *ival = (const V *)val;
-  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  // entries: thread t covers [t*K, t*K + K) within each sweep
-  for (int64_t e0 = t * kPackItems; e0 < nnz; e0 += stride * kPackItems) {
-    int64_t lo = 0, hi = len;  // last r in [0, len) with ptr[r] <= e0
-    while (hi - lo > 1) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (int64_t(ptr[mid]) <= e0) lo = mid; else hi = mid;
-    }
-    int64_t r = lo;
-    int64_t rend = ptr[r + 1];
-    const int64_t e1 = e0 + kPackItems < nnz ? e0 + kPackItems : nnz;
-    for (int64_t e = e0; e < e1; ++e) {
-      while (e >= rend) {
-        ++r;
-        rend = ptr[r + 1];
-      }
-      if ((mask[r >> 3] >> (r & 7)) & 1) {
-        const int64_t o = newp[r] + (e - int64_t(ptr[r]));
-        oval[o] = ival[e];
-        oidx[o] = idx[e];
-      }
-    }
-  }
-  // pointer array of the packed tile
-  PT *optr = (PT *)(out + ((kept * (VB + 4) + int64_t(sizeof(PT)) - 1) &
-                           ~(int64_t(sizeof(PT)) - 1)));
-  for (int64_t i = t; i <= len; i += stride) optr[i] = PT(newp[i]);
-  if (t == 0 && kept_dev) *kept_dev = kept;
 }
 
 template <typename PT>

@@ -54,6 +54,7 @@ extern "C" const char *tspg_strerror(int status) {
     case TSPG_ETIMEOUT: return "bounded device wait timed out";
     case TSPG_ECUDA: return "CUDA runtime error";
     case TSPG_EUNSORTED: return "operand rows must be sorted";
+    case TSPG_ESCRATCH: return "tile exceeds the static scratch of tspg_pack_noalloc";
     default: return "unknown status";
   }
 }
