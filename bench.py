@@ -44,7 +44,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="rmat", choices=["rmat", "uniform"])
+    p.add_argument("--workload", default="rmat", choices=["rmat", "uniform", "batched", "rap"])
+    p.add_argument("--products", type=int, default=512)
     p.add_argument("--scale", type=int, default=20)
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--seed", type=int, default=1)
@@ -388,8 +389,166 @@ def run_reference(args):
             "e2e": {"value": round(v, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ---------------------------------------------------------------- batched
+def run_batched(args):
+    """512 independent products C_i = A_i B_i (rows log-uniform in [1k, 200k],
+    Poisson row lengths with mean U[8, 32]): one batched run (two persistent
+    launches in two CUDA graphs) against a loop of plain tspg_spgemm calls."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from trident_b200 import ops, workloads
+    from trident_b200._lib import TSPG_F_B_SORTED, TspgCsrOut, check, lib
+    torch.cuda.set_device(0)
+    specs = workloads.batched_specs(args.products, seed=args.seed)
+    ctx = ops.Context(0)
+    dev, mults = [], 0
+    for spec in specs:
+        A, B = workloads.batched_product(spec)
+        dA, dB = A.to_device(), B.to_device()
+        dev.append((dA, dB))
+    bt = ops.Batch(ctx)
+    for dA, dB in dev:
+        bt.add(dA, dB)
+    stream = torch.cuda.current_stream()
+    total_nnz = bt.run(TSPG_F_B_SORTED)
+    for dA, dB in dev:
+        mults += ops.spgemm_count(ctx, dA, dB)[0]
+    for _ in range(args.warmup):
+        bt.run(TSPG_F_B_SORTED)
+    torch.cuda.synchronize()
+    l0 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(l0))
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        bt.run(TSPG_F_B_SORTED)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    l1 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(l1))
+    ms = e0.elapsed_time(e1) / args.steps
+    # the same products as a loop of plain calls (output buffer reused)
+    maxnnz = max(int(bt.result(i).nnz) for i in range(len(dev)))
+    maxrows = max(dA.nrows for dA, _ in dev)
+    Crp = torch.empty(maxrows + 1, dtype=torch.int64, device="cuda")
+    Ccol = torch.empty(max(maxnnz, 1), dtype=torch.int32, device="cuda")
+    Cval = torch.empty(max(maxnnz, 1), dtype=torch.float64, device="cuda")
+
+    def loop():
+        for dA, dB in dev:
+            a, b = dA.abi(), dB.abi()
+            o = TspgCsrOut()
+            o.nrows, o.ncols = dA.nrows, dB.ncols
+            o.rowptr, o.rowptr_bits, o.val_bits = Crp.data_ptr(), 64, 64
+            o.col, o.val, o.capacity = Ccol.data_ptr(), Cval.data_ptr(), maxnnz
+            check(lib.tspg_spgemm(ctx.h, stream.cuda_stream, C.byref(a), C.byref(b), C.byref(o),
+                                  TSPG_F_B_SORTED), "tspg_spgemm")
+    loop()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    loop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    loop_ms = e0.elapsed_time(e1)
+    n = len(dev)
+    line = {
+        "metric": "batched products/s (512 independent FP64 A_i B_i, one persistent launch per phase)",
+        "value": round(n / (ms * 1e-3), 1), "unit": "products/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poisson-row matrices, values U[-1,1])",
+        "config": {"workload": f"batched{n}", "products": n, "rows_total": int(sum(d[0].nrows for d in dev)),
+                   "nnz_A_total": int(sum(d[0].nnz for d in dev)), "mults": int(mults),
+                   "nnz_C_total": int(total_nnz), "rows": "log-uniform [1e3, 2e5]", "lambda": "U[8, 32]"},
+        "gflops": round(2.0 * mults / (ms * 1e-3) / 1e9, 3),
+        "loop_of_plain_calls": {"ms": round(loop_ms, 3), "products_per_s": round(n / (loop_ms * 1e-3), 1)},
+        "speedup_vs_loop": round(loop_ms / ms, 3),
+        "gpu_launches": int(l1.value - l0.value),
+        "clocks": clk,
+    }
+    bt.close()
+    ctx.close()
+    return line
+
+
+def run_rap(args):
+    """AMG Galerkin product on the 27-point Laplacian of an n^3 grid (n = 128 by
+    default, --scale sets n): AP = A·P, then RAP = R·(AP), R = P^T built by an
+    untimed host transpose.  One step = both products."""
+    import ctypes as C
+
+    import torch
+
+    from trident_b200 import ops, workloads
+    from trident_b200._lib import TSPG_F_B_SORTED, TspgCsrOut, check, lib
+    n = args.scale if args.scale != 20 else 128
+    torch.cuda.set_device(0)
+    R, A, P = workloads.galerkin_operands(n=n, pts=27, agg=3)
+    ctx = ops.Context(0)
+    dR, dA, dP = R.to_device(), A.to_device(), P.to_device()
+    m1 = ops.spgemm_count(ctx, dA, dP)[0]
+    AP = ops.spgemm(ctx, dA, dP, rowptr_bits=32)
+    m2 = ops.spgemm_count(ctx, dR, AP)[0]
+    RAP = ops.spgemm(ctx, dR, AP, rowptr_bits=32)
+    stream = torch.cuda.current_stream()
+
+    def call(X, Y, Cout):
+        x, y = X.abi(), Y.abi()
+        o = TspgCsrOut()
+        o.nrows, o.ncols = X.nrows, Y.ncols
+        o.rowptr, o.rowptr_bits, o.val_bits = Cout.rowptr.data_ptr(), 32, 64
+        o.col, o.val, o.capacity = Cout.col.data_ptr(), Cout.val.data_ptr(), Cout.nnz
+        check(lib.tspg_spgemm(ctx.h, stream.cuda_stream, C.byref(x), C.byref(y), C.byref(o), TSPG_F_B_SORTED),
+              "tspg_spgemm")
+
+    def step():
+        call(dA, dP, AP)
+        call(dR, AP, RAP)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_ap = 0.0
+    e0.record(stream)
+    for _ in range(args.steps):
+        ea.record(stream)
+        call(dA, dP, AP)
+        eb.record(stream)
+        call(dR, AP, RAP)
+        torch.cuda.synchronize()
+        t_ap += ea.elapsed_time(eb)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    ap_ms = t_ap / args.steps
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    bap = csr_bytes(A.nrows, A.nnz, 4) + csr_bytes(P.nrows, P.nnz, 4) + csr_bytes(AP.nrows, AP.nnz, 4)
+    brap = csr_bytes(R.nrows, R.nnz, 4) + csr_bytes(AP.nrows, AP.nnz, 4) + csr_bytes(RAP.nrows, RAP.nnz, 4)
+    line = {
+        "metric": "Galerkin R·A·P GFLOP/s (2 x multiply-adds), FP64", "value": round(2.0 * (m1 + m2) / (ms * 1e-3) / 1e9, 3),
+        "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic (27-point Laplacian, SA prolongator)",
+        "config": {"workload": f"rap27pt_{n}^3", "nnz_A": A.nnz, "nnz_P": P.nnz, "nnz_AP": AP.nnz, "nnz_RAP": RAP.nnz,
+                   "mults_AP": int(m1), "mults_RAP": int(m2)},
+        "AP": {"ms": round(ap_ms, 3), "hbm_frac": round(bap / (ap_ms * 1e-3) / 1e9 / peak, 4)},
+        "RAP": {"ms": round(ms - ap_ms, 3), "hbm_frac": round(brap / ((ms - ap_ms) * 1e-3) / 1e9 / peak, 4)},
+    }
+    ctx.close()
+    return line
+
+
 def main():
     args = parse()
+    if args.impl == "ours" and args.workload in ("batched", "rap"):
+        print(json.dumps(run_batched(args) if args.workload == "batched" else run_rap(args)), flush=True)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":

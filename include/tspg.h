@@ -182,6 +182,15 @@ int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
                     const tspg_csr *B, const tspg_csr *C_in,
                     tspg_csr_out *C_out, int flags);
 
+/* tspg_transpose — T = M^T with sorted rows (T is the CSC of M).  Replaces
+ * cusparse_csc_to_csr (include/cusparse_helpers.cuh:607-705) and
+ * LocalMatrix::csc_to_csr (include/KokkosWrap.hpp:442-531): a CSC tile
+ * passed as the CSR of its transpose comes back as the CSR of the tile.
+ * T->nrows = M->ncols, T->ncols = M->nrows; output capacity / allocator as
+ * for SpGEMM.  Synchronises `stream` once. */
+int tspg_transpose(tspg_ctx *ctx, void *stream, const tspg_csr *M,
+                   tspg_csr_out *T);
+
 /* ---- merge ------------------------------------------------------------------
  * tspg_spadd — C = A + B, union pattern, alpha = beta = 1.  Replaces
  * cusparse_spgeam (include/cusparse_helpers.cuh:799-905) and

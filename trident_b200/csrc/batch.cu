@@ -91,6 +91,10 @@ struct tspg_batch {
   int64_t *h_offs = nullptr;  // pinned, cap_prod + 1
   size_t h_offs_cap = 0;
   cudaGraphExec_t g1 = nullptr, g2 = nullptr;
+  // graphs are captured and launched on a batch-private stream (capture is
+  // not allowed on the legacy default stream); events join it to the caller's
+  cudaStream_t own = nullptr;
+  cudaEvent_t join_in = nullptr, join_out = nullptr;
   int g1_kernels = 0, g2_kernels = 0;
   cudaStream_t gstream = nullptr;
   bool dirty = true;
@@ -128,6 +132,26 @@ static int regrow(tspg_ctx *ctx, T **p, int64_t count, cudaStream_t s) {
   TSPG_TRY(ws_alloc(ctx, &q, size_t(count > 0 ? count : 1) * sizeof(T), s));
   *p = (T *)q;
   return TSPG_OK;
+}
+
+template <typename PT, typename VT>
+static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags);
+
+// Join the caller's stream to the batch stream, run, and join back.
+template <typename PT, typename VT>
+static int batch_run_joined(tspg_batch *b, cudaStream_t caller, int flags) {
+  tspg_ctx *ctx = b->ctx;
+  if (!b->own) {
+    TSPG_CUDA(ctx, cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
+    TSPG_CUDA(ctx, cudaEventCreateWithFlags(&b->join_in, cudaEventDisableTiming));
+    TSPG_CUDA(ctx, cudaEventCreateWithFlags(&b->join_out, cudaEventDisableTiming));
+  }
+  TSPG_CUDA(ctx, cudaEventRecord(b->join_in, caller));
+  TSPG_CUDA(ctx, cudaStreamWaitEvent(b->own, b->join_in, 0));
+  const int st = batch_run_impl<PT, VT>(b, b->own, flags);
+  TSPG_CUDA(ctx, cudaEventRecord(b->join_out, b->own));
+  TSPG_CUDA(ctx, cudaStreamWaitEvent(caller, b->join_out, 0));
+  return st;
 }
 
 template <typename PT, typename VT>
@@ -331,6 +355,9 @@ extern "C" int tspg_batch_destroy(tspg_batch *b) {
   b->drop_graphs();
   b->free_dev(nullptr);
   if (b->h_offs) cudaFreeHost(b->h_offs);
+  if (b->join_in) cudaEventDestroy(b->join_in);
+  if (b->join_out) cudaEventDestroy(b->join_out);
+  if (b->own) cudaStreamDestroy(b->own);
   delete b;
   return TSPG_OK;
 }
@@ -372,10 +399,10 @@ extern "C" int tspg_batch_run(tspg_batch *b, void *stream, int flags, int64_t *t
   TSPG_CUDA(b->ctx, cudaSetDevice(b->ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
   int st;
-  if (b->pt_bits == 32 && b->vt_bits == 64) st = batch_run_impl<int32_t, double>(b, s, flags);
-  else if (b->pt_bits == 64 && b->vt_bits == 64) st = batch_run_impl<int64_t, double>(b, s, flags);
-  else if (b->pt_bits == 32) st = batch_run_impl<int32_t, float>(b, s, flags);
-  else st = batch_run_impl<int64_t, float>(b, s, flags);
+  if (b->pt_bits == 32 && b->vt_bits == 64) st = batch_run_joined<int32_t, double>(b, s, flags);
+  else if (b->pt_bits == 64 && b->vt_bits == 64) st = batch_run_joined<int64_t, double>(b, s, flags);
+  else if (b->pt_bits == 32) st = batch_run_joined<int32_t, float>(b, s, flags);
+  else st = batch_run_joined<int64_t, float>(b, s, flags);
   if (st == TSPG_OK && total_nnz) *total_nnz = b->total_nnz;
   return st;
 }

@@ -208,7 +208,7 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
-  const int S = subgroup_width(f, a1 - a0, G);
+  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
   int cnt = 0;
   for_products_balanced<G, false, PT, VT>(
       P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane, gid, gm.lst, gm.nl, gm.cap,
@@ -229,7 +229,7 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t n = P.n;
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
-  const int S = subgroup_width(A.rowf[rr.g], a1 - a0, 32);
+  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, 32);
   const int64_t W = n < kDenseBits ? n : kDenseBits;
   int64_t total = 0;
   for (int64_t w0 = 0; w0 < n; w0 += W) {
@@ -367,7 +367,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
-  const int S = subgroup_width(A.rowf[rr.g], a1 - a0, G);
+  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
   for_products_balanced<G, true, PT, VT>(
       P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl,
       gm.cap, [&](int32_t col, VT v) {
@@ -472,7 +472,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   uint16_t *wp = (uint16_t *)(smem + size_t(nw) * 4);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
   const int64_t f = A.rowf[rr.g];
-  const int S = subgroup_width(f, a1 - a0, 32);
+  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, 32);
   for (int i = tid; i < nw; i += kThreads) bm[i] = 0u;
   __syncthreads();
   for_products_balanced<kThreads, false, PT, VT>(
@@ -550,7 +550,7 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const VT *__restrict__ Bx = P.Bx;
   // sub-group width from the per-window segment length of an average B row
   const int64_t nwin = (n + kDenseW - 1) / kDenseW;
-  const int S = subgroup_width(f / nwin, na, 32);
+  const int S = subgroup_width_avg(f / nwin, na, 32);
   const int sl = lane % S;
   const int subid = tid / S, nsub = kThreads / S;
   const unsigned submask =
@@ -701,25 +701,56 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   gm.nl = sh.nl + (G == 32 ? 12 + gid : slot);
   gm.cap = G;
   const int64_t base = sh.off[cls], count = sh.cnt[cls];
+  // rows are taken in chunks (one counter atomic per chunk); the chunk shrinks
+  // to one row as the class runs out so the tail stays balanced
+  constexpr int64_t kChunk = G == 32 ? 16 : G == 128 ? 4 : 2;
+  const int64_t groups = int64_t(gridDim.x) * (kThreads / G);
   while (true) {
     int64_t i;
     if constexpr (G == 32) {
       unsigned long long v = 0;
-      if (lane == 0) v = atomicAdd(&A.S->next[cls], 1ull);
-      i = (int64_t)__shfl_sync(0xffffffffu, v, 0);
+      if (lane == 0) {
+        const unsigned long long cur = *(volatile unsigned long long *)&A.S->next[cls];
+        const int64_t left = count - int64_t(cur);
+        const unsigned long long take =
+            left > kChunk * groups * 2 ? kChunk : 1ull;
+        v = atomicAdd(&A.S->next[cls], take) | (take << 48);
+      }
+      v = __shfl_sync(0xffffffffu, v, 0);
+      i = int64_t(v & ((1ull << 48) - 1));
+      const int64_t take = int64_t(v >> 48);
+      if (i >= count) break;
+      const int64_t e = min(count, i + take);
+      for (; i < e; ++i) {
+        const long long t0 = clock64();
+        if constexpr (NUM)
+          num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+        else
+          sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+        prof_add(A, cls, t0, lane == 0);
+      }
     } else {
-      if (lane == 0) sh.slot[slot] = atomicAdd(&A.S->next[cls], 1ull);
+      if (lane == 0) {
+        const unsigned long long cur = *(volatile unsigned long long *)&A.S->next[cls];
+        const int64_t left = count - int64_t(cur);
+        const unsigned long long take = left > kChunk * groups * 2 ? kChunk : 1ull;
+        sh.slot[slot] = atomicAdd(&A.S->next[cls], take) | (take << 48);
+      }
       group_sync<G>(gid);
-      i = (int64_t)sh.slot[slot];
+      const unsigned long long v = sh.slot[slot];
       group_sync<G>(gid);
+      i = int64_t(v & ((1ull << 48) - 1));
+      if (i >= count) break;
+      const int64_t e = min(count, i + int64_t(v >> 48));
+      for (; i < e; ++i) {
+        const long long t0 = clock64();
+        if constexpr (NUM)
+          num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+        else
+          sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+        prof_add(A, cls, t0, lane == 0);
+      }
     }
-    if (i >= count) break;
-    const long long t0 = clock64();
-    if constexpr (NUM)
-      num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
-    else
-      sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
-    prof_add(A, cls, t0, lane == 0);
   }
 }
 

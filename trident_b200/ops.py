@@ -180,6 +180,20 @@ def spadd(ctx: Context, A: DeviceCSR, B: DeviceCSR, rowptr_bits: int = 64, strea
 spgeam = spadd
 
 
+def transpose(ctx: Context, M: DeviceCSR, rowptr_bits: int = 64, stream=None) -> DeviceCSR:
+    """T = M^T, rows sorted (csc_to_csr: a CSC tile is the CSR of its transpose)."""
+    rp = torch.empty(M.ncols + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64,
+                     device=M.rowptr.device)
+    alloc = _TorchAlloc(M.rowptr.device)
+    o = _out_struct(M.ncols, M.nrows, rp, M.val_bits, alloc=alloc)
+    m = M.abi()
+    check(lib.tspg_transpose(ctx.h, _stream_ptr(stream), C.byref(m), C.byref(o)), "tspg_transpose")
+    return _finish(o, rp, alloc, M.val_bits)
+
+
+csc_to_csr = transpose
+
+
 def gen_bitmask(ctx: Context, ptr: torch.Tensor, n: int, stream=None) -> torch.Tensor:
     """Bit i of the mask = segment i of ptr non-empty (SpaComm::gen_bitmask, MASK_SIZE 8)."""
     out = torch.empty(max((n + 7) // 8, 1), dtype=torch.uint8, device=ptr.device)
@@ -232,6 +246,87 @@ def unpack(buf: torch.Tensor, nrows: int, ncols: int, nnz: int, major: int = TSP
     return DeviceCSR(nrows, ncols, rp, col, val, nnz=nnz)
 
 
-__all__ = ["Context", "Plan", "spgemm", "spgemm_count", "sp_mma", "spadd", "spgeam", "gen_bitmask",
+__all__ = ["Context", "Plan", "spgemm", "spgemm_count", "sp_mma", "spadd", "spgeam", "transpose",
+           "csc_to_csr", "gen_bitmask",
            "intersect_bitmasks", "compress", "unpack", "packed_bytes", "TSPG_ROWS", "TSPG_COLS",
            "TspgError", "TSPG_OK", "TSPG_ENOMEM"]
+
+
+class Batch:
+    """Many independent products in one persistent launch per phase
+    (tspg_batch_*).  Operands are borrowed: keep the DeviceCSR objects alive."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(lib.tspg_batch_create(ctx.h, C.byref(h)), "tspg_batch_create")
+        self.h = h
+        self._keep = []
+
+    def add(self, A: DeviceCSR, B: DeviceCSR) -> int:
+        a, b = A.abi(), B.abi()
+        i = C.c_int()
+        check(lib.tspg_batch_add(self.h, C.byref(a), C.byref(b), C.byref(i)), "tspg_batch_add")
+        self._keep.append((A, B))
+        return i.value
+
+    def clear(self):
+        check(lib.tspg_batch_clear(self.h), "tspg_batch_clear")
+        self._keep = []
+
+    def run(self, flags: int = 0, stream=None) -> int:
+        tot = C.c_int64()
+        check(lib.tspg_batch_run(self.h, _stream_ptr(stream), flags, C.byref(tot)), "tspg_batch_run")
+        return tot.value
+
+    def result(self, i: int) -> DeviceCSR:
+        """Result i as a DeviceCSR whose tensors alias the batch's output slab."""
+        v = TspgCsr()
+        check(lib.tspg_batch_result(self.h, i, C.byref(v)), "tspg_batch_result")
+        return _alias_csr(v)
+
+    def __len__(self):
+        return len(self._keep)
+
+    def close(self):
+        if self.h:
+            lib.tspg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _alias_csr(v: TspgCsr) -> DeviceCSR:
+    """Zero-copy torch views over device arrays owned by the library."""
+    nnz = int(v.nnz)
+    vdt = _vdtype(v.val_bits)
+    rdt = torch.int32 if v.rowptr_bits == 32 else torch.int64
+    rp = _device_view(v.rowptr, int(v.nrows) + 1, rdt)
+    col = _device_view(v.col, max(nnz, 1), torch.int32) if nnz else torch.empty(1, dtype=torch.int32, device="cuda")
+    val = _device_view(v.val, max(nnz, 1), vdt) if nnz else torch.empty(1, dtype=vdt, device="cuda")
+    return DeviceCSR(int(v.nrows), int(v.ncols), rp, col, val, nnz=nnz)
+
+
+def _device_view(ptr: int, count: int, dtype) -> torch.Tensor:
+    """A torch tensor over `count` elements of library-owned device memory."""
+    itemsize = torch.empty(0, dtype=dtype).element_size()
+
+    class _Arr:
+        __cuda_array_interface__ = {
+            "shape": (count,),
+            "typestr": {torch.int32: "<i4", torch.int64: "<i8", torch.float64: "<f8",
+                        torch.float32: "<f4"}[dtype],
+            "data": (int(ptr), False),
+            "version": 3,
+        }
+
+    t = torch.as_tensor(_Arr(), device="cuda")
+    assert t.element_size() == itemsize
+    return t
+
+
+__all__ += ["Batch"]
