@@ -263,9 +263,10 @@ int tspg_unpack(const void *buf, int64_t nrows, int64_t ncols, int major,
  * captured on the first run and replayed while the batch is unchanged.
  * Outputs go to one slab owned by the batch (context pool, reused across
  * runs); read each result with tspg_batch_result, valid until the next run,
- * clear or destroy.  All products of a batch share the rowptr and value
- * widths.  The batch borrows its operands: they must stay valid and
- * unchanged in shape while it is used. */
+ * clear or destroy.  All products of a batch share the value width; row
+ * offsets may mix int32 and int64 (the batch then runs with int64 offsets).
+ * The batch borrows its operands: they must stay valid and unchanged in
+ * shape while it is used. */
 typedef struct tspg_batch tspg_batch;
 int tspg_batch_create(tspg_ctx *ctx, tspg_batch **out);
 int tspg_batch_destroy(tspg_batch *b);
@@ -277,6 +278,39 @@ int tspg_batch_run(tspg_batch *b, void *stream, int flags,
                    int64_t *total_nnz);
 /* View of result i (device pointers into the batch's slab, int64 rowptr). */
 int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out);
+
+/* ---- serving ---------------------------------------------------------------------
+ * A continuous-batching server for C = A·B and Galerkin C = R·(A·P) requests
+ * with device-resident operands (borrowed until the request completes).
+ * Every request is admitted against `mem_budget` bytes by the upper bound on
+ * its output from the flop-count pass; admitted requests wait in a FIFO, and
+ * each of `lanes` worker threads (own context and stream) takes all waiting
+ * requests (up to max_batch) whenever it frees up and runs them as one
+ * batched product per stage, so batches formed while others run overlap on
+ * the device.  Results (int64 row offsets) stay valid until release. */
+enum { TSPG_REQ_AB = 0, TSPG_REQ_RAP = 1 };
+typedef struct tspg_server tspg_server;
+typedef struct tspg_server_config {
+  size_t mem_budget; /* admission budget, bytes */
+  int lanes;         /* concurrent worker lanes (1..16) */
+  int max_batch;     /* requests per batch */
+} tspg_server_config;
+/* The server uses ctx's device; it creates its own contexts and streams. */
+int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
+                       tspg_server **out);
+int tspg_server_destroy(tspg_server *s);
+/* kind TSPG_REQ_AB: C = A·B (R unused); TSPG_REQ_RAP: C = R·(A·B) with B the
+ * prolongator.  Returns TSPG_ENOMEM when the request alone exceeds the
+ * budget.  Thread-safe. */
+int tspg_server_submit(tspg_server *s, int kind, const tspg_csr *A,
+                       const tspg_csr *B, const tspg_csr *R, int64_t *ticket);
+/* Wait up to timeout_ms (< 0: forever) for a ticket; TSPG_ETIMEOUT if not
+ * done.  latency_ms = completion - submission (host clock). */
+int tspg_server_wait(tspg_server *s, int64_t ticket, int timeout_ms,
+                     tspg_csr *result, double *latency_ms);
+int tspg_server_release(tspg_server *s, int64_t ticket);
+int tspg_server_stats(tspg_server *s, int64_t *batches, int64_t *completed,
+                      int64_t *queued, size_t *reserved);
 
 /* ---- synthetic inputs (host) -----------------------------------------------------
  * Seeded generators of the benchmark operands, host memory, int64 rowptr.

@@ -81,3 +81,22 @@ def test_batch_with_empty_products(ctx):
     assert b.result(1).rowptr.cpu().tolist() == [0] * 8
     check_product(b.result(2), A, B)
     b.close()
+
+
+def test_batch_reuse_grows_rows_not_nnz(ctx):
+    # a second composition with more rows but fewer nonzeros reuses the slab
+    b = ops.Batch(ctx)
+    A1 = workloads.poisson_rows(2000, 30.0, 1)
+    d1 = (A1.to_device(), A1.to_device())
+    b.add(*d1)
+    b.run()
+    check_product(b.result(0), A1, A1)
+    b.clear()
+    A2 = workloads.poisson_rows(30000, 1.5, 2)
+    d2 = (A2.to_device(), A2.to_device())
+    b.add(*d2)
+    b.add(*d1)
+    b.run()
+    check_product(b.result(0), A2, A2)
+    check_product(b.result(1), A1, A1)
+    b.close()

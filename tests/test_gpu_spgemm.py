@@ -174,3 +174,13 @@ def test_dense_rows_wide_b_windowed(ctx):
     check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
     Bu = random_csr(3000, n, per_row=40, seed=23, sort=False)
     check_product(ops.spgemm(ctx, A.to_device(), Bu.to_device()), A, Bu)
+
+
+def test_mixed_rowptr_widths(ctx):
+    A = random_csr(300, 200, density=0.05, seed=30)
+    B = random_csr(200, 250, density=0.05, seed=31)
+    check_product(ops.spgemm(ctx, A.to_device(rowptr_bits=32), B.to_device(rowptr_bits=64)), A, B)
+    check_product(ops.spgemm(ctx, A.to_device(rowptr_bits=64), B.to_device(rowptr_bits=32)), A, B)
+    p = ops.Plan(ctx, A.to_device(rowptr_bits=32), B.to_device(rowptr_bits=64))
+    check_product(p.numeric(A.to_device(rowptr_bits=32), B.to_device(rowptr_bits=64)), A, B)
+    p.close()

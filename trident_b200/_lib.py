@@ -50,6 +50,13 @@ class TspgCsrOut(C.Structure):
     ]
 
 
+class TspgServerConfig(C.Structure):
+    _fields_ = [("mem_budget", C.c_size_t), ("lanes", C.c_int), ("max_batch", C.c_int)]
+
+
+TSPG_REQ_AB, TSPG_REQ_RAP = 0, 1
+
+
 class TspgHostCsr(C.Structure):
     _fields_ = [
         ("nrows", C.c_int64),
@@ -107,6 +114,12 @@ def _load() -> C.CDLL:
         "tspg_packed_bytes": (sz, [i64, i64, i32, i32]),
         "tspg_pack_noalloc": (i32, [vp, P(TspgCsr), i32, vp, vp, sz, vp]),
         "tspg_unpack": (i32, [vp, i64, i64, i32, i64, i32, i32, P(TspgCsr)]),
+        "tspg_server_create": (i32, [vp, P(TspgServerConfig), P(vp)]),
+        "tspg_server_destroy": (i32, [vp]),
+        "tspg_server_submit": (i32, [vp, i32, P(TspgCsr), P(TspgCsr), P(TspgCsr), P(i64)]),
+        "tspg_server_wait": (i32, [vp, i64, i32, P(TspgCsr), P(C.c_double)]),
+        "tspg_server_release": (i32, [vp, i64]),
+        "tspg_server_stats": (i32, [vp, P(i64), P(i64), P(i64), P(sz)]),
         "tspg_host_free": (None, [P(TspgHostCsr)]),
         "tspg_gen_uniform_rows": (i32, [i64, i32, i32, C.c_uint64, P(TspgHostCsr)]),
         "tspg_gen_rmat": (i32, [i32, i32, C.c_double, C.c_double, C.c_double, C.c_uint64, P(TspgHostCsr)]),

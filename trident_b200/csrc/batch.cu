@@ -87,6 +87,8 @@ struct tspg_batch {
   int32_t *Cj = nullptr;
   void *Cx = nullptr;
   int64_t *Cp = nullptr;
+  int64_t *wide = nullptr;  // int32 row offsets widened when the batch runs as int64
+  int64_t cap_wide = 0, cap_cp = 0;
   int64_t cap_rows = 0, cap_nnz = 0, cap_cur = 0, cap_prod = 0;
   int64_t *h_offs = nullptr;  // pinned, cap_prod + 1
   size_t h_offs_cap = 0;
@@ -106,7 +108,7 @@ struct tspg_batch {
   }
   void free_dev(cudaStream_t s) {
     void *ps[] = {prods, d_base, d_bbase, rowf, cp, partial, offs, rowc, list, sched,
-                  curbuf, Cj, Cx, Cp};
+                  curbuf, Cj, Cx, Cp, wide};
     for (void *p : ps) ws_free(ctx, p, s);
     prods = nullptr;
     d_base = d_bbase = rowf = cp = partial = offs = nullptr;
@@ -117,7 +119,8 @@ struct tspg_batch {
     Cj = nullptr;
     Cx = nullptr;
     Cp = nullptr;
-    cap_rows = cap_nnz = cap_cur = cap_prod = 0;
+    wide = nullptr;
+    cap_rows = cap_nnz = cap_cur = cap_prod = cap_wide = cap_cp = 0;
     prods_bytes = 0;
   }
 };
@@ -197,13 +200,41 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       TSPG_CUDA(ctx, cudaMallocHost((void **)&b->h_offs, sizeof(int64_t) * (nprod + 4)));
       b->h_offs_cap = nprod + 1;
     }
+    // operands with int32 offsets in an int64 batch are widened first
+    int64_t nwide = 0;
+    if (sizeof(PT) == 8)
+      for (int p = 0; p < nprod; ++p) {
+        if (b->A[p].rowptr_bits == 32) nwide += b->A[p].nrows + 1;
+        if (b->B[p].rowptr_bits == 32) nwide += b->B[p].nrows + 1;
+      }
+    if (nwide > b->cap_wide) {
+      TSPG_TRY(regrow(ctx, &b->wide, nwide, s));
+      b->cap_wide = nwide;
+    }
+    std::vector<const void *> arow(nprod), brow(nprod);
+    int64_t wo = 0;
+    for (int p = 0; p < nprod; ++p) {
+      const tspg_csr *M[2] = {&b->A[p], &b->B[p]};
+      const void **dst[2] = {&arow[p], &brow[p]};
+      for (int t = 0; t < 2; ++t) {
+        *dst[t] = M[t]->rowptr;
+        if (sizeof(PT) == 8 && M[t]->rowptr_bits == 32) {
+          const int64_t n = M[t]->nrows + 1;
+          k_widen<<<(unsigned)((n + 255) / 256), 256, 0, s>>>((const int32_t *)M[t]->rowptr, n,
+                                                              b->wide + wo);
+          ctx->launches += 1;
+          *dst[t] = b->wide + wo;
+          wo += n;
+        }
+      }
+    }
     std::vector<ProdDev<PT, VT>> hp(nprod);
     for (int p = 0; p < nprod; ++p) {
       ProdDev<PT, VT> v{};
-      v.Ap = (const PT *)b->A[p].rowptr;
+      v.Ap = (const PT *)arow[p];
       v.Aj = b->A[p].col;
       v.Ax = (const VT *)b->A[p].val;
-      v.Bp = (const PT *)b->B[p].rowptr;
+      v.Bp = (const PT *)brow[p];
       v.Bj = b->B[p].col;
       v.Bx = (const VT *)b->B[p].val;
       v.m = b->A[p].nrows;
@@ -286,12 +317,16 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
 
   // ---- output slab and graph 2: numeric
   bool regraph = rebuild;
-  if (b->total_nnz > b->cap_nnz || !b->Cp) {
+  if (b->total_nnz > b->cap_nnz || !b->Cj) {
     const int64_t nnz = b->total_nnz > 0 ? b->total_nnz : 1;
     TSPG_TRY(regrow(ctx, &b->Cj, nnz, s));
     TSPG_TRY(regrow(ctx, (VT **)&b->Cx, nnz, s));
-    TSPG_TRY(regrow(ctx, &b->Cp, R + nprod, s));
     b->cap_nnz = nnz;
+    regraph = true;
+  }
+  if (R + nprod > b->cap_cp || !b->Cp) {  // one row-offset array per product
+    TSPG_TRY(regrow(ctx, &b->Cp, R + nprod, s));
+    b->cap_cp = R + nprod;
     regraph = true;
   }
   if (b->max_a_row > kDenseCurSmem && b->max_a_row > b->cap_cur) {
@@ -376,12 +411,12 @@ extern "C" int tspg_batch_add(tspg_batch *b, const tspg_csr *A, const tspg_csr *
   if (!b) return TSPG_EINVAL;
   TSPG_TRY(check_csr(A));
   TSPG_TRY(check_csr(B));
-  if (A->ncols != B->nrows || A->val_bits != B->val_bits || A->rowptr_bits != B->rowptr_bits)
-    return TSPG_EINVAL;
-  if (!b->A.empty() && (A->rowptr_bits != b->pt_bits || A->val_bits != b->vt_bits))
-    return TSPG_EINVAL;
+  if (A->ncols != B->nrows || A->val_bits != B->val_bits) return TSPG_EINVAL;
+  if (!b->A.empty() && A->val_bits != b->vt_bits) return TSPG_EINVAL;
   if (b->A.size() >= (size_t(1) << 23) || A->nrows >= (int64_t(1) << 40)) return TSPG_EINVAL;
-  b->pt_bits = A->rowptr_bits;
+  // the batch runs with int64 offsets as soon as any operand has them
+  if (b->A.empty()) b->pt_bits = 32;
+  if (A->rowptr_bits == 64 || B->rowptr_bits == 64) b->pt_bits = 64;
   b->vt_bits = A->val_bits;
   if (index_out) *index_out = (int)b->A.size();
   b->A.push_back(*A);

@@ -16,6 +16,7 @@ namespace tspg {
 
 int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s) {
   bytes = (bytes + 255) & ~size_t(255);
+  std::lock_guard<std::mutex> lk(ctx->live_mu);
   if (ctx->budget && ctx->in_use + bytes > ctx->budget) return TSPG_ENOMEM;
   cudaError_t e = cudaMallocFromPoolAsync(p, bytes, ctx->pool, s);
   if (e != cudaSuccess) {
@@ -31,6 +32,7 @@ int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s) {
 
 void ws_free(tspg_ctx *ctx, void *p, cudaStream_t s) {
   if (!p) return;
+  std::lock_guard<std::mutex> lk(ctx->live_mu);
   auto it = ctx->live.find(p);
   if (it != ctx->live.end()) {
     ctx->in_use -= it->second;

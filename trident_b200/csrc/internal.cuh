@@ -25,6 +25,7 @@ struct tspg_ctx {
   // device words: error flag and small counters that live with the context
   int64_t *d_words = nullptr;
   std::unordered_map<void *, size_t> live;
+  std::mutex live_mu;  // ws_alloc / ws_free may be called from a releasing thread
   // instrumentation
   int64_t launches = 0;        // library kernels launched (graph nodes included)
   bool phase_timing = false;   // record events around the persistent phases

@@ -1,0 +1,371 @@
+// serve.cpp — continuous-batching server for A·B and Galerkin R·A·P requests.
+//
+// Requests arrive on any host thread (tspg_server_submit) with device-resident
+// operands.  Each is admitted against a device-memory budget by the upper
+// bound on its output from the flop-count pass (sum_i min(mults_i, ncols), 12
+// bytes per entry plus row offsets); requests wait in a FIFO until the budget
+// allows.  `lanes` worker threads, each with its own context, stream and two
+// tspg_batch objects, take every admitted request that is waiting when the
+// lane frees up (up to max_batch) and run them as one batched product per
+// stage: stage 1 = all A·B requests plus the A·P half of the R·A·P requests,
+// stage 2 = R·(AP) for the R·A·P requests.  Lanes run concurrently on their
+// own streams, so a batch that forms while others are on the GPU overlaps
+// with them.  Results are copied out of the batch slab into per-request
+// buffers from the lane's pool, which stay valid until tspg_server_release.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "tspg.h"
+
+namespace tspg {
+int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
+void ws_free(tspg_ctx *ctx, void *p, cudaStream_t s);
+}  // namespace tspg
+
+namespace {
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Req {
+  int64_t ticket = 0;
+  int kind = TSPG_REQ_AB;
+  tspg_csr A{}, B{}, R{};
+  size_t reserve = 0;  // admitted bytes
+  double t_submit = 0, t_start = 0, t_done = 0;
+  int status = TSPG_OK;
+  bool done = false;
+  // result (device, from the owning lane's pool)
+  int lane = -1;
+  int64_t nrows = 0, ncols = 0, nnz = 0;
+  int64_t *rp = nullptr;
+  int32_t *col = nullptr;
+  void *val = nullptr;
+};
+
+}  // namespace
+
+struct tspg_server {
+  int device = 0;
+  tspg_server_config cfg{};
+  tspg_ctx *adm = nullptr;  // admission context (count pass), used under mu
+  cudaStream_t adm_stream = nullptr;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Req *> queue;
+  std::unordered_map<int64_t, Req *> reqs;
+  size_t reserved = 0;
+  bool stop = false;
+  int64_t next_ticket = 1;
+  std::vector<std::thread> threads;
+  std::vector<tspg_ctx *> lane_ctx;
+  std::vector<cudaStream_t> lane_stream;
+  int64_t batches = 0, completed = 0, rejected = 0;
+  int lane_error = TSPG_OK;
+};
+
+namespace {
+
+size_t out_bytes(int64_t nnz_upper, int64_t rows, int vb) {
+  return size_t(nnz_upper) * size_t(4 + vb) + size_t(rows + 1) * 8;
+}
+
+// Copy batch result i into request-owned buffers from the lane pool.
+int take_result(tspg_ctx *ctx, cudaStream_t s, tspg_batch *b, int i, Req *r, int vb) {
+  tspg_csr v{};
+  int st = tspg_batch_result(b, i, &v);
+  if (st != TSPG_OK) return st;
+  r->nrows = v.nrows;
+  r->ncols = v.ncols;
+  r->nnz = v.nnz;
+  void *rp = nullptr, *col = nullptr, *val = nullptr;
+  st = tspg::ws_alloc(ctx, &rp, size_t(v.nrows + 1) * 8, s);
+  if (st == TSPG_OK) st = tspg::ws_alloc(ctx, &col, size_t(v.nnz > 0 ? v.nnz : 1) * 4, s);
+  if (st == TSPG_OK) st = tspg::ws_alloc(ctx, &val, size_t(v.nnz > 0 ? v.nnz : 1) * vb, s);
+  if (st != TSPG_OK) return st;
+  r->rp = (int64_t *)rp;
+  r->col = (int32_t *)col;
+  r->val = val;
+  if (cudaMemcpyAsync(rp, v.rowptr, size_t(v.nrows + 1) * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return TSPG_ECUDA;
+  if (v.nnz > 0) {
+    if (cudaMemcpyAsync(col, v.col, size_t(v.nnz) * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(val, v.val, size_t(v.nnz) * vb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return TSPG_ECUDA;
+  }
+  return TSPG_OK;
+}
+
+void lane_main(tspg_server *S, int lane) {
+  cudaSetDevice(S->device);
+  tspg_ctx *ctx = S->lane_ctx[lane];
+  cudaStream_t s = S->lane_stream[lane];
+  tspg_batch *b1 = nullptr, *b2 = nullptr;
+  tspg_batch_create(ctx, &b1);
+  tspg_batch_create(ctx, &b2);
+  std::vector<Req *> take;
+  while (true) {
+    take.clear();
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      if (S->stop && S->queue.empty()) break;
+      // FIFO admission by the memory budget; the head request is always
+      // admitted when nothing else is reserved (it was checked to fit alone)
+      while (!S->queue.empty() && (int)take.size() < S->cfg.max_batch) {
+        Req *r = S->queue.front();
+        if (S->reserved + r->reserve > S->cfg.mem_budget && !(S->reserved == 0 && take.empty()))
+          break;
+        S->queue.pop_front();
+        S->reserved += r->reserve;
+        take.push_back(r);
+      }
+      if (take.empty()) {
+        // budget held by other lanes: wait for a release
+        S->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+        continue;
+      }
+    }
+    const double t0 = now_ms();
+    for (Req *r : take) r->t_start = t0;
+    int st = TSPG_OK;
+    int vb = take[0]->A.val_bits / 8;
+    // stage 1: A·B and A·P
+    tspg_batch_clear(b1);
+    for (Req *r : take) {
+      int idx = 0;
+      if (st == TSPG_OK) st = tspg_batch_add(b1, &r->A, &r->B, &idx);
+    }
+    int64_t tot = 0;
+    if (st == TSPG_OK) st = tspg_batch_run(b1, s, 0, &tot);
+    // stage 2: R·(AP)
+    std::vector<int> rap;
+    if (st == TSPG_OK) {
+      tspg_batch_clear(b2);
+      for (int i = 0; i < (int)take.size() && st == TSPG_OK; ++i) {
+        if (take[i]->kind != TSPG_REQ_RAP) continue;
+        tspg_csr ap{};
+        st = tspg_batch_result(b1, i, &ap);
+        int idx = 0;
+        if (st == TSPG_OK) st = tspg_batch_add(b2, &take[i]->R, &ap, &idx);
+        rap.push_back(i);
+      }
+      if (st == TSPG_OK && !rap.empty()) st = tspg_batch_run(b2, s, 0, &tot);
+    }
+    if (st == TSPG_OK) {
+      for (int i = 0, k = 0; i < (int)take.size() && st == TSPG_OK; ++i) {
+        Req *r = take[i];
+        if (r->kind == TSPG_REQ_RAP) st = take_result(ctx, s, b2, k++, r, vb);
+        else st = take_result(ctx, s, b1, i, r, vb);
+        r->lane = lane;
+      }
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess && st == TSPG_OK) st = TSPG_ECUDA;
+    const double t1 = now_ms();
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      for (Req *r : take) {
+        r->status = st;
+        r->t_done = t1;
+        r->done = true;
+        if (st != TSPG_OK) {
+          S->reserved -= r->reserve;
+          r->reserve = 0;
+        }
+      }
+      S->batches += 1;
+      S->completed += int64_t(take.size());
+      if (st != TSPG_OK) S->lane_error = st;
+    }
+    S->cv_done.notify_all();
+  }
+  tspg_batch_destroy(b1);
+  tspg_batch_destroy(b2);
+}
+
+}  // namespace
+
+extern "C" int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
+                                  tspg_server **out) {
+  if (!ctx || !cfg || !out || cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1 ||
+      cfg->mem_budget == 0)
+    return TSPG_EINVAL;
+  *out = nullptr;
+  tspg_server *S = new (std::nothrow) tspg_server();
+  if (!S) return TSPG_ENOMEM;
+  S->cfg = *cfg;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  S->device = dev;
+  int st = tspg_ctx_create(dev, 0, &S->adm);
+  if (st == TSPG_OK && cudaStreamCreateWithFlags(&S->adm_stream, cudaStreamNonBlocking) != cudaSuccess)
+    st = TSPG_ECUDA;
+  for (int l = 0; l < cfg->lanes && st == TSPG_OK; ++l) {
+    tspg_ctx *c = nullptr;
+    cudaStream_t ls = nullptr;
+    st = tspg_ctx_create(dev, 0, &c);
+    if (st == TSPG_OK && cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking) != cudaSuccess)
+      st = TSPG_ECUDA;
+    S->lane_ctx.push_back(c);
+    S->lane_stream.push_back(ls);
+  }
+  if (st != TSPG_OK) {
+    tspg_server_destroy(S);
+    return st;
+  }
+  for (int l = 0; l < cfg->lanes; ++l) S->threads.emplace_back(lane_main, S, l);
+  *out = S;
+  return TSPG_OK;
+}
+
+extern "C" int tspg_server_destroy(tspg_server *S) {
+  if (!S) return TSPG_EINVAL;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_work.notify_all();
+  for (auto &t : S->threads) t.join();
+  cudaSetDevice(S->device);
+  cudaDeviceSynchronize();
+  for (auto &kv : S->reqs) {
+    Req *r = kv.second;
+    if (r->lane >= 0) {
+      tspg::ws_free(S->lane_ctx[r->lane], r->rp, nullptr);
+      tspg::ws_free(S->lane_ctx[r->lane], r->col, nullptr);
+      tspg::ws_free(S->lane_ctx[r->lane], r->val, nullptr);
+    }
+    delete r;
+  }
+  for (Req *r : S->queue)
+    if (!S->reqs.count(r->ticket)) delete r;
+  for (size_t l = 0; l < S->lane_ctx.size(); ++l) {
+    if (S->lane_stream[l]) cudaStreamDestroy(S->lane_stream[l]);
+    if (S->lane_ctx[l]) tspg_ctx_destroy(S->lane_ctx[l]);
+  }
+  if (S->adm_stream) cudaStreamDestroy(S->adm_stream);
+  if (S->adm) tspg_ctx_destroy(S->adm);
+  delete S;
+  return TSPG_OK;
+}
+
+extern "C" int tspg_server_submit(tspg_server *S, int kind, const tspg_csr *A,
+                                  const tspg_csr *B, const tspg_csr *R, int64_t *ticket) {
+  if (!S || !A || !B || !ticket) return TSPG_EINVAL;
+  if (kind != TSPG_REQ_AB && kind != TSPG_REQ_RAP) return TSPG_EINVAL;
+  if (kind == TSPG_REQ_RAP && !R) return TSPG_EINVAL;
+  Req *r = new (std::nothrow) Req();
+  if (!r) return TSPG_ENOMEM;
+  r->kind = kind;
+  r->A = *A;
+  r->B = *B;
+  if (R) r->R = *R;
+  r->t_submit = now_ms();
+  std::lock_guard<std::mutex> lk(S->mu);
+  // admission bound from the count pass: the A·B output, or A·P plus R·A·P
+  // (bounded by rows(R) x ncols(P)) for the Galerkin product
+  int64_t mults = 0, upper = 0;
+  cudaSetDevice(S->device);
+  int st = tspg_spgemm_count(S->adm, S->adm_stream, A, B, &mults, &upper);
+  if (st != TSPG_OK) {
+    delete r;
+    return st;
+  }
+  const int vb = A->val_bits / 8;
+  size_t bytes = out_bytes(upper, A->nrows, vb);
+  if (kind == TSPG_REQ_RAP) {
+    const int64_t full = R->nrows * B->ncols;
+    const int64_t up2 = std::min<int64_t>(full, upper > 0 ? R->nnz * (upper / std::max<int64_t>(1, A->nrows) + 1) : 0);
+    bytes += out_bytes(up2, R->nrows, vb);
+  }
+  r->reserve = bytes;
+  if (bytes > S->cfg.mem_budget) {
+    delete r;
+    S->rejected += 1;
+    return TSPG_ENOMEM;
+  }
+  r->ticket = S->next_ticket++;
+  S->reqs[r->ticket] = r;
+  S->queue.push_back(r);
+  *ticket = r->ticket;
+  S->cv_work.notify_one();
+  return TSPG_OK;
+}
+
+extern "C" int tspg_server_wait(tspg_server *S, int64_t ticket, int timeout_ms,
+                                tspg_csr *result, double *latency_ms) {
+  if (!S) return TSPG_EINVAL;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->reqs.find(ticket);
+  if (it == S->reqs.end()) return TSPG_EINVAL;
+  Req *r = it->second;
+  const auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms);
+  while (!r->done) {
+    if (timeout_ms >= 0) {
+      if (S->cv_done.wait_until(lk, deadline) == std::cv_status::timeout && !r->done)
+        return TSPG_ETIMEOUT;
+    } else {
+      S->cv_done.wait(lk);
+    }
+  }
+  if (latency_ms) *latency_ms = r->t_done - r->t_submit;
+  if (r->status != TSPG_OK) return r->status;
+  if (result) {
+    result->nrows = r->nrows;
+    result->ncols = r->ncols;
+    result->nnz = r->nnz;
+    result->rowptr = r->rp;
+    result->rowptr_bits = 64;
+    result->val_bits = r->A.val_bits;
+    result->col = r->col;
+    result->val = r->val;
+  }
+  return TSPG_OK;
+}
+
+extern "C" int tspg_server_release(tspg_server *S, int64_t ticket) {
+  if (!S) return TSPG_EINVAL;
+  Req *r = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end() || !it->second->done) return TSPG_EINVAL;
+    r = it->second;
+    S->reqs.erase(it);
+    S->reserved -= r->reserve;
+  }
+  if (r->lane >= 0) {
+    // the lane's pool is stream-ordered on the lane stream; its work on these
+    // buffers finished before the request was marked done
+    tspg::ws_free(S->lane_ctx[r->lane], r->rp, S->lane_stream[r->lane]);
+    tspg::ws_free(S->lane_ctx[r->lane], r->col, S->lane_stream[r->lane]);
+    tspg::ws_free(S->lane_ctx[r->lane], r->val, S->lane_stream[r->lane]);
+  }
+  delete r;
+  S->cv_work.notify_all();
+  S->cv_done.notify_all();
+  return TSPG_OK;
+}
+
+extern "C" int tspg_server_stats(tspg_server *S, int64_t *batches, int64_t *completed,
+                                 int64_t *queued, size_t *reserved) {
+  if (!S) return TSPG_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (batches) *batches = S->batches;
+  if (completed) *completed = S->completed;
+  if (queued) *queued = int64_t(S->queue.size());
+  if (reserved) *reserved = S->reserved;
+  return S->lane_error;
+}

@@ -55,6 +55,7 @@ struct tspg_plan {
   int64_t nb = 0;
   int32_t *curbuf = nullptr;
   int64_t cur_stride = 0;
+  int64_t *wide_a = nullptr, *wide_b = nullptr;  // widened row offsets (mixed widths)
   void *blocks[16];
   int nblocks = 0;
 
@@ -210,7 +211,6 @@ static int check_pair(const tspg_csr *A, const tspg_csr *B) {
   TSPG_TRY(check_csr(B));
   if (A->ncols != B->nrows) return TSPG_EINVAL;
   if (A->val_bits != B->val_bits) return TSPG_EINVAL;
-  if (A->rowptr_bits != B->rowptr_bits) return TSPG_EINVAL;
   return TSPG_OK;
 }
 
@@ -240,19 +240,39 @@ extern "C" int tspg_plan_destroy(tspg_plan *plan) {
   return TSPG_OK;
 }
 
+static int plan_get(tspg_ctx *, void *plan, int64_t **p, int64_t n) {
+  return ((tspg_plan *)plan)->get(p, size_t(n));
+}
+
 extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
-                                    const tspg_csr *A, const tspg_csr *B,
+                                    const tspg_csr *A_in, const tspg_csr *B_in,
                                     int flags, tspg_plan **plan,
                                     int64_t *c_nnz) {
   if (!ctx || !plan) return TSPG_EINVAL;
   *plan = nullptr;
-  TSPG_TRY(check_pair(A, B));
+  TSPG_TRY(check_pair(A_in, B_in));
   cudaStream_t s = (cudaStream_t)stream;
   TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
   tspg_plan *P = new (std::nothrow) tspg_plan();
   if (!P) return TSPG_ENOMEM;
   P->ctx = ctx;
   P->stream = s;
+  tspg_csr a = *A_in, b = *B_in;
+  const tspg_csr *A = &a, *B = &b;
+  if (a.rowptr_bits != b.rowptr_bits) {
+    tspg_csr *M = a.rowptr_bits == 32 ? &a : &b;
+    int64_t **buf = M == &a ? &P->wide_a : &P->wide_b;
+    int st = P->get(buf, size_t(M->nrows + 1));
+    if (st != TSPG_OK) {
+      delete P;
+      return st;
+    }
+    k_widen<<<(unsigned)((M->nrows + 1 + 255) / 256), 256, 0, s>>>((const int32_t *)M->rowptr,
+                                                                    M->nrows + 1, *buf);
+    ctx->launches += 1;
+    M->rowptr = *buf;
+    M->rowptr_bits = 64;
+  }
   P->pt_bits = A->rowptr_bits;
   P->vt_bits = A->val_bits;
   int st = dispatch(P->pt_bits, P->vt_bits, [&](auto pt, auto vt) {
@@ -270,10 +290,22 @@ extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
 }
 
 extern "C" int tspg_spgemm_numeric(tspg_ctx *ctx, void *stream,
-                                   tspg_plan *plan, const tspg_csr *A,
-                                   const tspg_csr *B, tspg_csr_out *C) {
+                                   tspg_plan *plan, const tspg_csr *A_in,
+                                   const tspg_csr *B_in, tspg_csr_out *C) {
   if (!ctx || !plan) return TSPG_EINVAL;
-  TSPG_TRY(check_pair(A, B));
+  TSPG_TRY(check_pair(A_in, B_in));
+  tspg_csr a = *A_in, b = *B_in;
+  const tspg_csr *A = &a, *B = &b;
+  if (a.rowptr_bits != b.rowptr_bits) {
+    tspg_csr *M = a.rowptr_bits == 32 ? &a : &b;
+    int64_t *buf = M == &a ? plan->wide_a : plan->wide_b;
+    if (!buf) return TSPG_EINVAL;  // the symbolic call had matching widths
+    k_widen<<<(unsigned)((M->nrows + 1 + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        (const int32_t *)M->rowptr, M->nrows + 1, buf);
+    ctx->launches += 1;
+    M->rowptr = buf;
+    M->rowptr_bits = 64;
+  }
   if (A->nrows != plan->m || B->ncols != plan->n || A->nnz != plan->a_nnz ||
       B->nnz != plan->b_nnz || A->rowptr_bits != plan->pt_bits ||
       A->val_bits != plan->vt_bits)
@@ -334,11 +366,24 @@ extern "C" int tspg_spgemm_count(tspg_ctx *ctx, void *stream,
   TSPG_TRY(check_pair(A, B));
   cudaStream_t s = (cudaStream_t)stream;
   TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  Scratch sc(ctx, s);
+  tspg_csr a = *A, b = *B;
+  if (a.rowptr_bits != b.rowptr_bits) {
+    tspg_csr *M = a.rowptr_bits == 32 ? &a : &b;
+    int64_t *buf;
+    TSPG_TRY(sc.get(&buf, M->nrows + 1));
+    k_widen<<<(unsigned)((M->nrows + 1 + 255) / 256), 256, 0, s>>>((const int32_t *)M->rowptr,
+                                                                    M->nrows + 1, buf);
+    ctx->launches += 1;
+    M->rowptr = buf;
+    M->rowptr_bits = 64;
+  }
+  A = &a;
+  B = &b;
   return dispatch(A->rowptr_bits, A->val_bits, [&](auto pt, auto vt) -> int {
     using PT = std::remove_pointer_t<decltype(pt)>;
     using VT = std::remove_pointer_t<decltype(vt)>;
     const int64_t m = A->nrows;
-    Scratch sc(ctx, s);
     ProdDev<PT, VT> *prods;
     int64_t *base, *rowf;
     Sched *sched;

@@ -175,6 +175,12 @@ __global__ void k_set_prod(ProdDev<PT, VT> *dst, ProdDev<PT, VT> v,
   base[1] = m;
 }
 
+// int32 row offsets widened to int64 (operands of mixed offset widths).
+static __global__ void k_widen(const int32_t *src, int64_t n, int64_t *dst) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+
 // New operand arrays for a plan's numeric re-run; the sortedness found by the
 // symbolic pass is kept.
 template <typename PT, typename VT>

@@ -330,3 +330,57 @@ def _device_view(ptr: int, count: int, dtype) -> torch.Tensor:
 
 
 __all__ += ["Batch"]
+
+
+class Server:
+    """Continuous-batching server (tspg_server_*): A·B and R·(A·P) requests with
+    device-resident operands, admitted by the output upper bound."""
+
+    def __init__(self, ctx: Context, mem_budget: int, lanes: int = 2, max_batch: int = 64):
+        from ._lib import TspgServerConfig
+        cfg = TspgServerConfig(mem_budget, lanes, max_batch)
+        h = C.c_void_p()
+        check(lib.tspg_server_create(ctx.h, C.byref(cfg), C.byref(h)), "tspg_server_create")
+        self.h = h
+        self._ops = {}
+
+    def submit(self, A: DeviceCSR, B: DeviceCSR, R: DeviceCSR | None = None) -> int:
+        from ._lib import TSPG_REQ_AB, TSPG_REQ_RAP
+        a, b = A.abi(), B.abi()
+        r = R.abi() if R is not None else None
+        t = C.c_int64()
+        check(lib.tspg_server_submit(self.h, TSPG_REQ_RAP if R is not None else TSPG_REQ_AB, C.byref(a),
+                                     C.byref(b), C.byref(r) if r is not None else None, C.byref(t)),
+              "tspg_server_submit")
+        self._ops[t.value] = (A, B, R)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """(DeviceCSR view of the result, latency ms); valid until release()."""
+        v = TspgCsr()
+        lat = C.c_double()
+        check(lib.tspg_server_wait(self.h, ticket, timeout_ms, C.byref(v), C.byref(lat)), "tspg_server_wait")
+        return _alias_csr(v), lat.value
+
+    def release(self, ticket: int):
+        check(lib.tspg_server_release(self.h, ticket), "tspg_server_release")
+        self._ops.pop(ticket, None)
+
+    def stats(self):
+        b, c, q, r = C.c_int64(), C.c_int64(), C.c_int64(), C.c_size_t()
+        st = lib.tspg_server_stats(self.h, C.byref(b), C.byref(c), C.byref(q), C.byref(r))
+        return {"batches": b.value, "completed": c.value, "queued": q.value, "reserved": r.value, "status": st}
+
+    def close(self):
+        if self.h:
+            lib.tspg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ += ["Server"]
