@@ -135,12 +135,14 @@ int tspg_ctx_stats(const tspg_ctx *ctx, int64_t *launches);
 int tspg_ctx_phase_timing(tspg_ctx *ctx, int enable);
 int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
 /* Per-class accounting of the persistent phases (off by default): SM cycles
- * and rows per row class, accumulated over calls since enabling.  out28 =
- * symbolic[cycles x 7, rows x 7], numeric[cycles x 7, rows x 7]; classes in
- * order DENSE0 (>= 2^20 products), DENSE1 (>= 2^17), DENSE2, G1024, G256,
- * G128, G32.  Reading synchronises the device. */
+ * and rows per row class, accumulated over calls since enabling.  out64 =
+ * symbolic[32], numeric[32]; each half holds cycles x 7, rows x 7 (classes
+ * DENSE0 (>= 2^20 products), DENSE1 (>= 2^17), DENSE2, G1024, G256, G128,
+ * G32), then (numeric only) cycles of the whole-row DENSE rows' bitmap
+ * pass, column scan and value pass.  Reading synchronises the
+ * device. */
 int tspg_ctx_class_profile(tspg_ctx *ctx, int enable);
-int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out28);
+int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out64);
 
 /* ---- SpGEMM ----------------------------------------------------------------
  * tspg_spgemm_count — the flop-count pass.  mults = sum over A's nonzeros

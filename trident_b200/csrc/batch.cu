@@ -347,7 +347,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       k_scatter<PT, VT, 1><<<(unsigned)((R + 255) / 256), 256, 0, s>>>(
           prods, b->d_base, nprod, R, b->rowf, b->rowc, b->cp, b->sched + 1, b->list);
       PhaseArgs pa{b->d_base, b->sched + 1, b->list, b->rowf, b->rowc, b->cp,
-                   b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + 14 : nullptr};
+                   b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
       phase_mark(ctx, 1, 0, s);
       k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 1, 1, s);

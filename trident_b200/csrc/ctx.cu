@@ -178,8 +178,8 @@ extern "C" int tspg_ctx_class_profile(tspg_ctx *ctx, int enable) {
   if (!ctx) return TSPG_EINVAL;
   TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
   if (enable && !ctx->d_prof)
-    TSPG_CUDA(ctx, cudaMalloc((void **)&ctx->d_prof, 2 * 14 * sizeof(unsigned long long)));
-  if (enable) TSPG_CUDA(ctx, cudaMemset(ctx->d_prof, 0, 2 * 14 * sizeof(unsigned long long)));
+    TSPG_CUDA(ctx, cudaMalloc((void **)&ctx->d_prof, 64 * sizeof(unsigned long long)));
+  if (enable) TSPG_CUDA(ctx, cudaMemset(ctx->d_prof, 0, 64 * sizeof(unsigned long long)));
   if (!enable && ctx->d_prof) {
     cudaFree(ctx->d_prof);
     ctx->d_prof = nullptr;
@@ -187,9 +187,9 @@ extern "C" int tspg_ctx_class_profile(tspg_ctx *ctx, int enable) {
   return TSPG_OK;
 }
 
-extern "C" int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out28) {
-  if (!ctx || !ctx->d_prof || !out28) return TSPG_EINVAL;
+extern "C" int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out64) {
+  if (!ctx || !ctx->d_prof || !out64) return TSPG_EINVAL;
   TSPG_CUDA(ctx, cudaDeviceSynchronize());
-  TSPG_CUDA(ctx, cudaMemcpy(out28, ctx->d_prof, 28 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  TSPG_CUDA(ctx, cudaMemcpy(out64, ctx->d_prof, 64 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
   return TSPG_OK;
 }

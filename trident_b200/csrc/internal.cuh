@@ -216,4 +216,13 @@ __device__ __forceinline__ void set_error(int64_t *err, int code) {
   atomicCAS((unsigned long long *)err, 0ull, (unsigned long long)code);
 }
 
+// Fire-and-forget global reduction (PTX `red`): no value comes back, so the
+// issuing thread never waits on the L2 round trip.
+__device__ __forceinline__ void red_add(double *p, double v) {
+  asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+__device__ __forceinline__ void red_add(float *p, float v) {
+  asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
 }  // namespace tspg

@@ -182,7 +182,7 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
       prods, P->base, 1, m, P->rowf, P->rowc, P->cp, P->sched + 1, P->list);
   PhaseArgs pa{P->base, P->sched + 1, P->list, P->rowf, P->rowc, P->cp,
                P->curbuf, P->cur_stride, ctx->d_words + kErrWord,
-               ctx->d_prof ? ctx->d_prof + 14 : nullptr};
+               ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
   phase_mark(ctx, 1, 0, s);
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
   phase_mark(ctx, 1, 1, s);

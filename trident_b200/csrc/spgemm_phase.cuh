@@ -24,7 +24,7 @@ template <bool NUM, typename VT, typename F>
 __device__ __forceinline__ void walk_row(const int32_t *__restrict__ Bj,
                                          const VT *__restrict__ Bx, int64_t q0,
                                          int64_t b1, int step, VT a, F &&fn) {
-  constexpr int U = 4;
+  constexpr int U = 8;
   for (int64_t q = q0; q < b1; q += int64_t(step) * U) {
     int32_t c[U];
     VT x[U];
@@ -157,12 +157,22 @@ struct PhaseArgs {
   unsigned long long *prof;  // optional: [class] cycles, [NCLS + class] rows
 };
 
-// Optional per-class accounting (SM cycles spent in each row class).
+// Optional per-class accounting (SM cycles spent in each row class), and
+// sub-phase cycles of the DENSE numeric rows at [kProfSub + i].
+constexpr int kProfSub = 2 * NCLS;
+constexpr int kProfPerPhase = 32;
 __device__ __forceinline__ void prof_add(const PhaseArgs &A, int cls, long long t0,
                                          bool leader) {
   if (A.prof && leader) {
     atomicAdd(A.prof + cls, (unsigned long long)(clock64() - t0));
     atomicAdd(A.prof + NCLS + cls, 1ull);
+  }
+}
+__device__ __forceinline__ void prof_sub(const PhaseArgs &A, int i, long long &t) {
+  if (A.prof && threadIdx.x == 0) {
+    const long long now = clock64();
+    atomicAdd(A.prof + kProfSub + i, (unsigned long long)(now - t));
+    t = now;
   }
 }
 
@@ -453,12 +463,12 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 }
 
 // DENSE numeric row, whole-row form (ncols <= kRankMaxCols).  Pass 1 sets the
-// row's column bitmap; a CTA scan of the bitmap gives every word's rank base
-// (per-thread chunk base + uint16 offset inside the chunk) and writes the
-// sorted column indices and zeroed values of the row's output; pass 2 adds
-// every product into its output slot, found as base + popc of the bits below,
-// with a global FP64 reduction (the row's output segment is L2-resident while
-// the CTA works on it).  No windows, no sort.
+// row's column bitmap; a striped CTA scan of the bitmap gives every word's
+// rank base and writes the sorted column indices and zeroed values of the
+// row's output with coalesced stores; pass 2 adds every product into its
+// output slot, found as base + popc of the bits below, with a global FP64
+// reduction (the row's output segment is L2-resident while the CTA works on
+// it).  No windows, no sort.
 template <typename PT, typename VT>
 __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                                    int64_t idx, unsigned char *smem, const GroupMem &gm,
@@ -470,52 +480,71 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   const int nw = int((n + 31) >> 5);
   uint32_t *bm = (uint32_t *)smem;
   uint16_t *wp = (uint16_t *)(smem + size_t(nw) * 4);
-  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1], na = a1 - a0;
   const int64_t f = A.rowf[rr.g];
-  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, 32);
+  const int32_t *__restrict__ Aj = P.Aj;
+  const VT *__restrict__ Ax = P.Ax;
+  const PT *__restrict__ Bp = P.Bp;
+  const int32_t *__restrict__ Bj = P.Bj;
+  const VT *__restrict__ Bx = P.Bx;
+  const int S1 = subgroup_width_avg(f, na, 32);
+  long long tp = clock64();
   for (int i = tid; i < nw; i += kThreads) bm[i] = 0u;
   __syncthreads();
   for_products_balanced<kThreads, false, PT, VT>(
-      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, tid, 0, gm.lst, gm.nl, gm.cap,
+      Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
       [&](int32_t col, VT) {
         const uint32_t bit = 1u << (col & 31);
         if (!(((volatile uint32_t *)bm)[col >> 5] & bit)) atomicOr(bm + (col >> 5), bit);
       });
   __syncthreads();
-  // chunk of 2^lc consecutive words per thread
-  int lc = 0;
-  while ((kThreads << lc) < nw) ++lc;
-  const int w0 = tid << lc, w1 = min(nw, (tid + 1) << lc);
-  int cnt = 0;
-  for (int w = w0; w < w1; ++w) cnt += __popc(bm[w]);
-  int64_t tot;
-  const int base = int(group_excl_scan<kThreads, int64_t>(int64_t(cnt), gm.tmp, 0, &tot));
-  tbase[tid] = base;
+  prof_sub(A, 0, tp);
+  // Striped scan: round r covers words [r*kRW, (r+1)*kRW); thread t owns
+  // words r*kRW + 2t and + 2t + 1, so consecutive threads write consecutive
+  // output ranks.  wp[w] = rank of word w's first bit within its round (at
+  // most 32768, fits uint16), tbase[r] = rank of round r's first bit.
+  constexpr int kRW = 2 * kThreads;
+  const int rounds = (nw + kRW - 1) / kRW;
   const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
   int32_t *__restrict__ Cj = P.Cj + off;
   VT *__restrict__ Cx = P.Cx + off;
-  int run = 0;
-  for (int w = w0; w < w1; ++w) {
-    uint32_t word = bm[w];
-    wp[w] = uint16_t(run);
-    while (word) {
-      const int b = __ffs(word) - 1;
-      word &= word - 1;
-      Cj[base + run] = int32_t(w * 32 + b);
-      Cx[base + run] = VT(0);
-      ++run;
+  int rbase = 0;
+  for (int r = 0; r < rounds; ++r) {
+    const int w = r * kRW + 2 * tid;
+    const uint32_t x0 = w < nw ? bm[w] : 0u, x1 = w + 1 < nw ? bm[w + 1] : 0u;
+    const int n0 = __popc(x0);
+    int64_t rtot;
+    const int pos =
+        int(group_excl_scan<kThreads, int64_t>(int64_t(n0 + __popc(x1)), gm.tmp, 0, &rtot));
+    if (w < nw) wp[w] = uint16_t(pos);
+    if (w + 1 < nw) wp[w + 1] = uint16_t(pos + n0);
+    if (tid == 0) tbase[r] = rbase;
+    int o = rbase + pos;
+    for (int h = 0; h < 2; ++h) {
+      uint32_t word = h ? x1 : x0;
+      const int cb = (w + h) * 32;
+      while (word) {
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        Cj[o] = cb + b;
+        Cx[o] = VT(0);
+        ++o;
+      }
     }
+    rbase += int(rtot);
   }
-  if (tid == 0 && tot != A.rowc[rr.g]) set_error(A.err, 104);
-  __threadfence();
   __syncthreads();
+  if (tid == 0 && rbase != A.rowc[rr.g]) set_error(A.err, 104);
+  prof_sub(A, 1, tp);
+  auto rank_of = [&](int32_t col) {
+    const int w = col >> 5;
+    return tbase[w / kRW] + int(wp[w]) + __popc(bm[w] & ((1u << (col & 31)) - 1u));
+  };
   for_products_balanced<kThreads, true, PT, VT>(
-      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, tid, 0, gm.lst, gm.nl, gm.cap,
-      [&](int32_t col, VT v) {
-        const int w = col >> 5;
-        const int rank = tbase[w >> lc] + int(wp[w]) + __popc(bm[w] & ((1u << (col & 31)) - 1u));
-        atomicAdd(Cx + rank, v);
-      });
+      Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
+      [&](int32_t col, VT v) { red_add(Cx + rank_of(col), v); });
+  __syncthreads();
+  prof_sub(A, 2, tp);
 }
 
 // DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry
