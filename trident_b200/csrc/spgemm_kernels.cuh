@@ -67,8 +67,9 @@ constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory
 constexpr int64_t kDenseBits = int64_t(kTableSmem + kCountSmem) * 8;  // whole-row bitmap
 constexpr int kBitonicMax = 64;          // rows up to this size sort bitonic
-// whole-row DENSE numeric form: bitmap (4 B) + uint16 rank offset per 32 columns
-constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 6) * 32;
+// whole-row DENSE numeric form: per 32 columns a bitmap word (4 B) and a
+// uint16 rank offset, per 1024 columns an int block base (196 B per block)
+constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 196) * 1024;
 
 __host__ __device__ inline int dense_sub(int64_t f) {
   return f >= (int64_t(1) << 20) ? CLS_DENSE0 : f >= (int64_t(1) << 17) ? CLS_DENSE1 : CLS_DENSE2;

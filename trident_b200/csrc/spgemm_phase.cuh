@@ -463,25 +463,30 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 }
 
 // DENSE numeric row, whole-row form (ncols <= kRankMaxCols).  Pass 1 sets the
-// row's column bitmap; a striped CTA scan of the bitmap gives every word's
-// rank base and writes the sorted column indices and zeroed values of the
-// row's output with coalesced stores; pass 2 adds every product into its
-// output slot, found as base + popc of the bits below, with a global FP64
-// reduction (the row's output segment is L2-resident while the CTA works on
-// it).  No windows, no sort.
+// row's column bitmap; a CTA scan of the bitmap gives every word's rank base
+// (block base + uint16 offset inside the block); the row's values are zeroed
+// (coalesced) and its sorted column indices written with the work balanced
+// by entries, not by words (R-MAT bitmaps are far denser at the hub columns);
+// pass 2 adds every product into its output slot, found as base + popc of the
+// bits below, with a fire-and-forget global FP64 reduction.  No sort.
 template <typename PT, typename VT>
 __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
-                                   int64_t idx, unsigned char *smem, const GroupMem &gm,
-                                   int *tbase) {
+                                   int64_t idx, unsigned char *smem, const GroupMem &gm) {
   const int tid = threadIdx.x;
   const RowRef rr = decode_row(A, idx);
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t n = P.n;
   const int nw = int((n + 31) >> 5);
+  const int nb = (nw + 31) >> 5;
+  // Bitmap word w lives at slot w ^ ((w >> 6) & 31): a bijection inside each
+  // 32-word block that spreads threads walking words ~64 apart over all banks.
   uint32_t *bm = (uint32_t *)smem;
-  uint16_t *wp = (uint16_t *)(smem + size_t(nw) * 4);
+  uint16_t *wp = (uint16_t *)(smem + size_t(nb) * 128);
+  int *bbase = (int *)(smem + size_t(nb) * 192);
+  auto bmw = [&](int w) -> uint32_t & { return bm[w ^ ((w >> 6) & 31)]; };
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1], na = a1 - a0;
   const int64_t f = A.rowf[rr.g];
+  const int64_t c = A.rowc[rr.g];
   const int32_t *__restrict__ Aj = P.Aj;
   const VT *__restrict__ Ax = P.Ax;
   const PT *__restrict__ Bp = P.Bp;
@@ -489,62 +494,107 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   const VT *__restrict__ Bx = P.Bx;
   const int S1 = subgroup_width_avg(f, na, 32);
   long long tp = clock64();
-  for (int i = tid; i < nw; i += kThreads) bm[i] = 0u;
+  for (int i = tid; i < nb * 32; i += kThreads) bm[i] = 0u;
   __syncthreads();
   for_products_balanced<kThreads, false, PT, VT>(
       Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
       [&](int32_t col, VT) {
         const uint32_t bit = 1u << (col & 31);
-        if (!(((volatile uint32_t *)bm)[col >> 5] & bit)) atomicOr(bm + (col >> 5), bit);
+        uint32_t &x = bmw(col >> 5);
+        if (!(*(volatile uint32_t *)&x & bit)) atomicOr(&x, bit);
       });
   __syncthreads();
   prof_sub(A, 0, tp);
-  // Striped scan: round r covers words [r*kRW, (r+1)*kRW); thread t owns
-  // words r*kRW + 2t and + 2t + 1, so consecutive threads write consecutive
-  // output ranks.  wp[w] = rank of word w's first bit within its round (at
-  // most 32768, fits uint16), tbase[r] = rank of round r's first bit.
-  constexpr int kRW = 2 * kThreads;
-  const int rounds = (nw + kRW - 1) / kRW;
+  // Block scan: block b = words [32b, 32b + 32), lane l of a warp takes word
+  // 32b + l (no bank conflicts).  wp[w] = rank of word w's first bit within
+  // its block (< 1024), bbase[b] = rank of block b's first bit.
+  {
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int b = warp; b < nb; b += kThreads / 32) {
+      const int w = (b << 5) + lane;
+      const int pc = w < nw ? __popc(bmw(w)) : 0;
+      const int inc = warp_scan_incl(pc);
+      if (w < nw) wp[w] = uint16_t(inc - pc);
+      if (lane == 31) bbase[b] = inc;
+    }
+  }
+  __syncthreads();
+  {
+    constexpr int BPT = 3;  // blocks per thread: nb <= kRankMaxCols / 1024 < 3 * kThreads
+    int v[BPT], sum = 0;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      const int b = tid * BPT + k;
+      v[k] = b < nb ? bbase[b] : 0;
+      sum += v[k];
+    }
+    int64_t tot;
+    // the scan ends on a barrier, so every read of bbase above is done
+    int run = int(group_excl_scan<kThreads, int64_t>(int64_t(sum), gm.tmp, 0, &tot));
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+      const int b = tid * BPT + k;
+      if (b < nb) bbase[b] = run;
+      run += v[k];
+    }
+    if (tid == 0 && tot != c) set_error(A.err, 104);
+  }
+  __syncthreads();
+  prof_sub(A, 1, tp);
   const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
   int32_t *__restrict__ Cj = P.Cj + off;
   VT *__restrict__ Cx = P.Cx + off;
-  int rbase = 0;
-  for (int r = 0; r < rounds; ++r) {
-    const int w = r * kRW + 2 * tid;
-    const uint32_t x0 = w < nw ? bm[w] : 0u, x1 = w + 1 < nw ? bm[w + 1] : 0u;
-    const int n0 = __popc(x0);
-    int64_t rtot;
-    const int pos =
-        int(group_excl_scan<kThreads, int64_t>(int64_t(n0 + __popc(x1)), gm.tmp, 0, &rtot));
-    if (w < nw) wp[w] = uint16_t(pos);
-    if (w + 1 < nw) wp[w + 1] = uint16_t(pos + n0);
-    if (tid == 0) tbase[r] = rbase;
-    int o = rbase + pos;
-    for (int h = 0; h < 2; ++h) {
-      uint32_t word = h ? x1 : x0;
-      const int cb = (w + h) * 32;
-      while (word) {
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        Cj[o] = cb + b;
-        Cx[o] = VT(0);
-        ++o;
+  // zeroed values: a contiguous range, coalesced
+  for (int64_t e = tid; e < c; e += kThreads) Cx[e] = VT(0);
+  prof_sub(A, 2, tp);
+  // Column indices.  The bitmap walk is a merge of two sequences, the words
+  // and the set bits (nw + c steps: every bit, then a step to the next word);
+  // thread t takes steps [d_t, d_t+1), d_t = t * (nw + c) / kThreads (merge-
+  // path split), so threads get equal work however the bits cluster, and the
+  // loop below takes exactly one step per iteration, so the lanes of a warp
+  // stay in step.  A split point is found by searching w + rank(w) over the
+  // block bases, then over the word offsets of one block.
+  {
+    const int64_t steps = int64_t(nw) + c;
+    const int64_t d0 = steps * tid / kThreads, d1 = steps * (tid + 1) / kThreads;
+    int lo = 0, hi = nb - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (int64_t(mid) * 32 + bbase[mid] <= d0) lo = mid; else hi = mid - 1;
+    }
+    int w = lo << 5, wh = min(nw, (lo + 1) << 5) - 1;
+    while (w < wh) {
+      const int mid = (w + wh + 1) >> 1;
+      if (int64_t(mid) + bbase[lo] + wp[mid] <= d0) w = mid; else wh = mid - 1;
+    }
+    int e = int(d0 - w);  // first rank of this thread
+    uint32_t word = bmw(w);
+    // the lowest e - rank(w) set bits of this word belong to earlier threads
+    for (int k = e - bbase[w >> 5] - int(wp[w]); k > 0; --k) word &= word - 1u;
+    uint32_t nxt = w + 1 < nw ? bmw(w + 1) : 0u;
+    for (int64_t d = d0; d < d1; ++d) {
+      if (word != 0u) {
+        if (e < c) Cj[e] = w * 32 + (__ffs(word) - 1);  // e < c unless rank sums broke
+        ++e;
+        word &= word - 1u;
+      } else {
+        ++w;
+        word = nxt;
+        nxt = w + 1 < nw ? bmw(w + 1) : 0u;
       }
     }
-    rbase += int(rtot);
   }
   __syncthreads();
-  if (tid == 0 && rbase != A.rowc[rr.g]) set_error(A.err, 104);
-  prof_sub(A, 1, tp);
+  prof_sub(A, 3, tp);
   auto rank_of = [&](int32_t col) {
     const int w = col >> 5;
-    return tbase[w / kRW] + int(wp[w]) + __popc(bm[w] & ((1u << (col & 31)) - 1u));
+    return bbase[w >> 5] + int(wp[w]) + __popc(bmw(w) & ((1u << (col & 31)) - 1u));
   };
   for_products_balanced<kThreads, true, PT, VT>(
       Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
       [&](int32_t col, VT v) { red_add(Cx + rank_of(col), v); });
   __syncthreads();
-  prof_sub(A, 2, tp);
+  prof_sub(A, 4, tp);
 }
 
 // DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry
@@ -789,7 +839,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ PhaseShared sh;
   __shared__ int64_t s_items[kCtaClasses + 1];
-  __shared__ int s_tbase[NUM ? kThreads : 1];
   const int tid = threadIdx.x;
   if (tid < NCLS) {
     sh.off[tid] = A.S->off[tid];
@@ -826,7 +875,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if constexpr (NUM) {
         const ProdDev<PT, VT> &P = prods[decode_row(A, idx).p];
         if (P.n <= kRankMaxCols)
-          num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm, s_tbase);
+          num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm);
         else
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);
       } else {
