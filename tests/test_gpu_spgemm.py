@@ -176,6 +176,23 @@ def test_dense_rows_wide_b_windowed(ctx):
     check_product(ops.spgemm(ctx, A.to_device(), Bu.to_device()), A, Bu)
 
 
+def test_dense_rows_wide_b_long_rows_global_cursors(ctx):
+    # windowed sweep with A rows longer than the shared cursor array (cursors
+    # in global scratch) and a few hub rows of B (walked by one warp each)
+    n = 1_200_000
+    rng = np.random.default_rng(24)
+    B = random_csr(12000, n, per_row=12, seed=25)
+    hub_rows = [3, 777, 5000, 11999]
+    rows = [np.sort(rng.choice(n, 6000, replace=False)) if i in hub_rows else
+            B.col[B.rowptr[i]:B.rowptr[i + 1]] for i in range(B.nrows)]
+    rp = np.zeros(B.nrows + 1, dtype=np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate(rows).astype(np.int32)
+    B = HostCSR(B.nrows, n, rp, col, rng.uniform(-1, 1, col.size))
+    A = random_csr(3, B.nrows, per_row=9000, seed=26)
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+
+
 def test_mixed_rowptr_widths(ctx):
     A = random_csr(300, 200, density=0.05, seed=30)
     B = random_csr(200, 250, density=0.05, seed=31)

@@ -330,7 +330,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
     regraph = true;
   }
   if (b->max_a_row > kDenseCurSmem && b->max_a_row > b->cap_cur) {
-    TSPG_TRY(regrow(ctx, &b->curbuf, int64_t(ctx->num_sms) * b->max_a_row, s));
+    TSPG_TRY(regrow(ctx, &b->curbuf, 2 * int64_t(ctx->num_sms) * b->max_a_row, s));
     b->cap_cur = b->max_a_row;
     b->cur_stride = b->max_a_row;
     regraph = true;

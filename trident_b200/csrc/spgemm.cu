@@ -175,7 +175,7 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
   }
   if (P->max_a_row > kDenseCurSmem && !P->curbuf) {
     P->cur_stride = P->max_a_row;
-    TSPG_TRY(P->get(&P->curbuf, size_t(ctx->num_sms) * P->cur_stride));
+    TSPG_TRY(P->get(&P->curbuf, 2 * size_t(ctx->num_sms) * P->cur_stride));
   }
   k_sched_offsets<<<1, 32, 0, s>>>(P->sched + 1);
   k_scatter<PT, VT, 1><<<grid_for(m, 256, INT32_MAX), 256, 0, s>>>(

@@ -151,7 +151,8 @@ struct PhaseArgs {
   const int64_t *rowf;
   int32_t *rowc;
   const int64_t *cp;
-  int32_t *curbuf;     // per-CTA cursor scratch for DENSE rows with long A rows
+  int32_t *curbuf;     // per-CTA cursor scratch for DENSE rows with long A rows:
+                       // 2 x cur_stride entries per CTA (cursor, column at it)
   int64_t cur_stride;  // entries per CTA in curbuf
   int64_t *err;
   unsigned long long *prof;  // optional: [class] cycles, [NCLS + class] rows
@@ -597,134 +598,152 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   prof_sub(A, 4, tp);
 }
 
-// DENSE numeric row: sweep the columns in windows of kDenseW.  Each A entry
-// keeps a cursor into its (sorted) B row, so every B entry is read once; the
-// window's accumulator is dense FP64 plus a presence bitmap, and the window is
-// emitted in column order.  B rows longer than a sub-group's fair share are
-// listed once per row; in each window their segment end is found by binary
-// search and the whole CTA walks the segment.  With unsorted B every window
-// rescans the rows (no cursors, no list).
+// DENSE numeric row, column windows of kDenseW.  Each window accumulates in
+// a dense shared FP64 array plus a presence bitmap (shared atomics, no global
+// reductions) and is emitted in column order, so a heavy row's output is
+// written once.  With sorted B every A entry keeps a cursor into its B row and
+// the first column at the cursor: an entry with nothing in the window costs
+// one shared load, and one thread walks an entry's window segment with U
+// loads in flight (stopping at the first column past the window).  B rows
+// longer than twice a thread's fair share are listed once per row and walked
+// by one warp each, U x 32 entries per step, with the same stop rule.  With
+// unsorted B every window rescans the rows.
 template <typename PT, typename VT>
 __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                               int64_t idx, unsigned char *smem, const GroupMem &gm) {
   constexpr int kLongMark = INT32_MIN;
-  const int tid = threadIdx.x, lane = tid & 31;
+  constexpr int U = 8;
+  const int tid = threadIdx.x;
   int64_t *scan_tmp = gm.tmp;
   VT *acc = (VT *)smem;
-  uint32_t *bm = (uint32_t *)(smem + kDenseW * 8);
-  int32_t *cur_s = (int32_t *)(smem + kDenseW * 8 + kDenseW / 8);
-  int32_t *lcur = cur_s + kDenseCurSmem;  // cursor of listed entry i
-  int32_t *lend = lcur + 1024;            // its segment end in this window
+  uint32_t *bm = (uint32_t *)(smem + kDenseW * sizeof(VT));
+  int32_t *cur_s = (int32_t *)(smem + kDenseW * sizeof(VT) + kDenseW / 8);
+  int32_t *lcur = cur_s + 2 * kDenseCurSmem;  // cursor of listed entry i
   const RowRef rr = decode_row(A, idx);
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t n = P.n;
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1], na = a1 - a0;
   const int64_t f = A.rowf[rr.g];
-  int32_t *cur = na <= kDenseCurSmem ? cur_s : A.curbuf + blockIdx.x * A.cur_stride;
+  // cursor (offset into the B row) and the column at the cursor, per A entry
+  int32_t *cur = na <= kDenseCurSmem ? cur_s : A.curbuf + 2 * blockIdx.x * A.cur_stride;
+  int32_t *nxc = na <= kDenseCurSmem ? cur_s + kDenseCurSmem : cur + A.cur_stride;
   const bool sorted = P.b_sorted != 0;
   const int32_t *__restrict__ Aj = P.Aj;
   const VT *__restrict__ Ax = P.Ax;
   const PT *__restrict__ Bp = P.Bp;
   const int32_t *__restrict__ Bj = P.Bj;
   const VT *__restrict__ Bx = P.Bx;
-  // sub-group width from the per-window segment length of an average B row
-  const int64_t nwin = (n + kDenseW - 1) / kDenseW;
-  const int S = subgroup_width_avg(f / nwin, na, 32);
-  const int sl = lane % S;
-  const int subid = tid / S, nsub = kThreads / S;
-  const unsigned submask =
-      S == 32 ? 0xffffffffu : (((1u << S) - 1u) << ((lane / S) * S));
-  const int64_t thr = max(int64_t(4 * S) * nwin, f / nsub);
+  const int64_t thr = max(int64_t(4 * U), 2 * f / kThreads);
+  long long tp = clock64();
+  auto add = [&](int32_t o, VT v) {
+    atomicAdd(acc + o, v);
+    const uint32_t bit = 1u << (o & 31);
+    if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
+  };
   if (tid == 0) *gm.nl = 0;
   for (int i = tid; i < kDenseW; i += kThreads) acc[i] = VT(0);
   for (int i = tid; i < kDenseW / 32; i += kThreads) bm[i] = 0u;
   __syncthreads();
-  // classify: listed (long) entries get the cursor mark
-  for (int64_t j = subid; j < na; j += nsub) {
-    int mark = 0;
-    if (sorted && sl == 0) {
+  if (sorted) {
+    for (int64_t j = tid; j < na; j += kThreads) {
       const int64_t k = __ldg(Aj + a0 + j);
-      if (__ldg(Bp + k + 1) - __ldg(Bp + k) > thr) {
+      const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+      int32_t c0 = 0, nc = b1 > b0 ? __ldg(Bj + b0) : INT32_MAX;
+      if (b1 - b0 > thr) {
         const int slot = atomicAdd(gm.nl, 1);
         if (slot < gm.cap) {
           gm.lst[slot] = int(j);
           lcur[slot] = 0;
-          mark = kLongMark;
+          c0 = kLongMark;
+          nc = INT32_MAX;
         }
       }
+      cur[j] = c0;
+      nxc[j] = nc;
     }
-    if (sl == 0) cur[j] = mark;
   }
   __syncthreads();
-  const int nl = min(*gm.nl, gm.cap);
+  const int nl = sorted ? min(*gm.nl, gm.cap) : 0;
+  prof_sub(A, 5, tp);
   int64_t out = A.cp[rr.g] - A.cp[A.base[rr.p]];
   for (int64_t w0 = 0; w0 < n; w0 += kDenseW) {
     const int64_t w1 = (w0 + kDenseW < n) ? w0 + kDenseW : n;
-    // segment ends of the listed entries in this window
-    for (int i = tid; i < nl; i += kThreads) {
-      const int64_t k = __ldg(Aj + a0 + gm.lst[i]);
-      int64_t lo = __ldg(Bp + k) + lcur[i], hi = __ldg(Bp + k + 1);
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (__ldg(Bj + mid) < w1) lo = mid + 1; else hi = mid;
-      }
-      lend[i] = int32_t(lo - __ldg(Bp + k));
-    }
-    // short entries: sub-groups with cursors
-    for (int64_t j = subid; j < na; j += nsub) {
+    // short entries: one thread per entry
+    for (int64_t j = tid; j < na; j += kThreads) {
+      if (sorted && nxc[j] >= w1) continue;  // nothing in this window (or listed)
       const int64_t k = __ldg(Aj + a0 + j);
       const VT a = __ldg(Ax + a0 + j);
       const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
       if (sorted) {
-        const int32_t c0 = cur[j];
-        if (c0 == kLongMark) continue;
-        int64_t q = b0 + c0;
+        int64_t q = b0 + cur[j];
+        int32_t ncol = INT32_MAX;
         while (q < b1) {
-          const int64_t qq = q + sl;
-          const bool valid = qq < b1;
-          const int32_t col = valid ? __ldg(Bj + qq) : INT32_MAX;
-          const bool in = valid && col < w1;
-          const unsigned bal = __ballot_sync(submask, in);
-          if (in) {
-            const uint32_t o = uint32_t(col - w0);
-            atomicAdd(acc + o, a * __ldg(Bx + qq));
-            const uint32_t bit = 1u << (o & 31);
-            if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
+          int32_t cc[U];
+          VT xv[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int64_t qq = q + u;
+            cc[u] = qq < b1 ? __ldg(Bj + qq) : INT32_MAX;
+            xv[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
           }
-          const int nin = __popc(bal);
+          int nin = 0;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (cc[u] < w1) {
+              add(int32_t(cc[u] - w0), a * xv[u]);
+              ++nin;
+            } else {
+              ncol = min(ncol, cc[u]);
+            }
+          }
           q += nin;
-          if (nin < S) break;
+          if (nin < U) break;
         }
-        if (sl == 0) cur[j] = int32_t(q - b0);
+        cur[j] = int32_t(q - b0);
+        nxc[j] = ncol;
       } else {
-        for (int64_t q = b0 + sl; q < b1; q += S) {
+        for (int64_t q = b0; q < b1; ++q) {
           const int32_t col = __ldg(Bj + q);
-          if (col >= w0 && col < w1) {
-            const uint32_t o = uint32_t(col - w0);
-            atomicAdd(acc + o, a * __ldg(Bx + q));
-            const uint32_t bit = 1u << (o & 31);
-            if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
-          }
+          if (col >= w0 && col < w1) add(int32_t(col - w0), a * __ldg(Bx + q));
         }
       }
     }
-    __syncthreads();  // lend[] ready
-    // long entries: the whole CTA walks [lcur, lend)
-    for (int i = 0; i < nl; ++i) {
+    if (A.prof) __syncthreads();  // profiling only: split short / long walks
+    prof_sub(A, 6, tp);
+    // long entries: warp w walks listed entries w, w + 16, ...; its lanes take
+    // U x 32 entries per step and stop at the first column past the window
+    for (int i = tid >> 5; i < nl; i += kThreads / 32) {
+      const int lane = tid & 31;
       const int64_t p = a0 + gm.lst[i];
       const int64_t k = __ldg(Aj + p);
       const VT a = __ldg(Ax + p);
-      const int64_t b0 = __ldg(Bp + k);
-      const int64_t e = b0 + lend[i];
-      walk_row<true, VT>(Bj, Bx, b0 + lcur[i] + tid, e, kThreads, a, [&](int32_t col, VT v) {
-        const uint32_t o = uint32_t(col - w0);
-        atomicAdd(acc + o, v);
-        const uint32_t bit = 1u << (o & 31);
-        if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
-      });
+      const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+      int64_t q = b0 + lcur[i];
+      while (q < b1) {
+        int32_t cc[U];
+        VT xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t qq = q + u * 32 + lane;
+          cc[u] = qq < b1 ? __ldg(Bj + qq) : INT32_MAX;
+          xv[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
+        }
+        int nin = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (cc[u] < w1) {
+            add(int32_t(cc[u] - w0), a * xv[u]);
+            ++nin;
+          }
+        }
+        nin = __reduce_add_sync(0xffffffffu, nin);
+        q += nin;
+        if (nin < U * 32) break;
+      }
+      if (lane == 0) lcur[i] = int32_t(q - b0);
     }
     __syncthreads();
-    for (int i = tid; i < nl; i += kThreads) lcur[i] = lend[i];
+    prof_sub(A, 7, tp);
     uint32_t word = tid < kDenseW / 32 ? bm[tid] : 0u;
     int64_t tot;
     int64_t pos = group_excl_scan<kThreads, int64_t>(int64_t(__popc(word)),
@@ -743,6 +762,7 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     if (tid < kDenseW / 32) bm[tid] = 0u;
     out += tot;
     __syncthreads();
+    prof_sub(A, 8, tp);
   }
 }
 
