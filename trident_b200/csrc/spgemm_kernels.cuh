@@ -57,11 +57,11 @@ __host__ __device__ constexpr bool cls_dense(int c) { return c <= CLS_DENSE2; }
 // key + FP64 value (192 KiB per CTA); a table has T = pow2 >= 2x the bound.
 __host__ __device__ constexpr int64_t kSymLim32 = 512, kSymLim128 = 2048,
                                       kSymLim256 = 4096, kSymLim1024 = 24576;
-__host__ __device__ constexpr int64_t kNumLim32 = 256, kNumLim128 = 1024,
+__host__ __device__ constexpr int64_t kNumLim32 = 512, kNumLim128 = 1024,
                                       kNumLim256 = 2048, kNumLim1024 = 8192;
 constexpr int kSymT32 = 1024, kSymT128 = 4096, kSymT256 = 8192,
               kSymT1024 = 32768;
-constexpr int kNumT32 = 512, kNumT128 = 2048, kNumT256 = 4096,
+constexpr int kNumT32 = 1024, kNumT128 = 2048, kNumT256 = 4096,
               kNumT1024 = 16384;
 constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory

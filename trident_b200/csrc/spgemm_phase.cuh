@@ -108,6 +108,84 @@ __device__ __forceinline__ void for_products_balanced(
   }
 }
 
+// Flat product loop for group rows.  A entries are taken G at a time: lane j
+// loads entry j's column, value and B row bounds, so a chunk's loads are all
+// in flight together; a group scan of the B row lengths numbers the chunk's
+// products and lanes take products lane, lane + G, ... (U per step, loads in
+// flight), each finding its entry as the last one whose first product number
+// is <= its own.  G = 32 keeps the per-entry data in registers (shuffles);
+// larger groups stage it in `stage` (24 bytes per lane of shared memory).
+template <int G, bool NUM, typename PT, typename VT, typename F>
+__device__ __forceinline__ void for_products_flat(
+    const int32_t *__restrict__ Aj, const VT *__restrict__ Ax,
+    const PT *__restrict__ Bp, const int32_t *__restrict__ Bj,
+    const VT *__restrict__ Bx, int64_t a0, int64_t a1, int lane, int gid,
+    int64_t *tmp, unsigned char *stage, F &&fn) {
+  constexpr int U = 4;
+  int64_t *spre = (int64_t *)stage;
+  int64_t *sb0 = spre + G;
+  VT *sa = (VT *)(sb0 + G);
+  for (int64_t c0 = a0; c0 < a1; c0 += G) {
+    const int nc = int(min(int64_t(G), a1 - c0));
+    int64_t len = 0, b0 = 0;
+    VT a = VT(0);
+    if (lane < nc) {
+      const int64_t k = __ldg(Aj + c0 + lane);
+      if constexpr (NUM) a = __ldg(Ax + c0 + lane);
+      b0 = __ldg(Bp + k);
+      len = __ldg(Bp + k + 1) - b0;
+    }
+    int64_t tot;
+    const int64_t pre = group_excl_scan<G, int64_t>(len, tmp, gid, &tot);
+    if constexpr (G != 32) {
+      if (lane < nc) {
+        spre[lane] = pre;
+        sb0[lane] = b0;
+        sa[lane] = a;
+      }
+      group_sync<G>(gid);
+    }
+    // the step loop is uniform across the group (the G = 32 search shuffles)
+    for (int64_t pb = 0; pb < tot; pb += int64_t(G) * U) {
+      int32_t cc[U];
+      VT xv[U], av[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t p = pb + int64_t(u) * G + lane;
+        int j = 0;
+        int64_t pj, bj;
+        if constexpr (G == 32) {
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const int64_t v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
+            if (j + st < nc && v <= p) j += st;
+          }
+          pj = __shfl_sync(0xffffffffu, pre, j);
+          bj = __shfl_sync(0xffffffffu, b0, j);
+          if constexpr (NUM) av[u] = __shfl_sync(0xffffffffu, a, j);
+        } else {
+          for (int st = G / 2; st > 0; st >>= 1)
+            if (j + st < nc && spre[j + st] <= p) j += st;
+          pj = spre[j];
+          bj = sb0[j];
+          if constexpr (NUM) av[u] = sa[j];
+        }
+        const int64_t q = bj + (p - pj);
+        cc[u] = p < tot ? __ldg(Bj + q) : -1;
+        if constexpr (NUM) xv[u] = p < tot ? __ldg(Bx + q) : VT(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (cc[u] >= 0) {
+          if constexpr (NUM) fn(cc[u], av[u] * xv[u]);
+          else fn(cc[u], VT(0));
+        }
+      }
+    }
+    group_sync<G>(gid);  // the next chunk reuses the staging
+  }
+}
+
 // Probe bound: tables are sized T >= 2 * (distinct keys), so a probe never
 // runs T steps; the bound only turns a broken invariant into an error flag.
 __device__ __forceinline__ int sym_insert(int *keys, int32_t col, int logT,
@@ -199,6 +277,7 @@ struct GroupMem {
   int *nl;        // their count
   int cap;        // list capacity
   uint16_t *cnt;  // radix digit counters
+  unsigned char *stage;  // flat product loop staging (G = 128 / 256), 24 B per lane
 };
 
 // ---------------------------------------------------------------- symbolic
@@ -219,11 +298,16 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
-  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
   int cnt = 0;
-  for_products_balanced<G, false, PT, VT>(
-      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane, gid, gm.lst, gm.nl, gm.cap,
-      [&](int32_t col, VT) { cnt += sym_insert(keys, col, logT, mask, A.err); });
+  auto ins = [&](int32_t col, VT) { cnt += sym_insert(keys, col, logT, mask, A.err); };
+  if constexpr (G <= 256) {
+    for_products_flat<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
+                                        gm.tmp, gm.stage, ins);
+  } else {
+    const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
+    for_products_balanced<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane,
+                                            gid, gm.lst, gm.nl, gm.cap, ins);
+  }
   group_sync<G>(gid);
   const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
   if (lane == 0) A.rowc[rr.g] = int32_t(total);
@@ -378,13 +462,19 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
-  const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
-  for_products_balanced<G, true, PT, VT>(
-      P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl,
-      gm.cap, [&](int32_t col, VT v) {
-        const uint32_t h = num_insert(keys, col, logT, mask, A.err);
-        atomicAdd(vals + h, v);
-      });
+  auto ins = [&](int32_t col, VT v) {
+    const uint32_t h = num_insert(keys, col, logT, mask, A.err);
+    atomicAdd(vals + h, v);
+  };
+  if constexpr (G <= 256) {
+    for_products_flat<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
+                                       gm.tmp, gm.stage, ins);
+  } else {
+    const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
+    for_products_balanced<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
+                                           A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl, gm.cap,
+                                           ins);
+  }
   group_sync<G>(gid);
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
   // so first-half slots are held in registers across the group barrier inside
@@ -793,12 +883,19 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const int slot = G == 256 ? gid : G == 128 ? 4 + gid : 0;
   unsigned char *slice = smem + gid * SLICE;
   GroupMem gm;
-  gm.cnt = (uint16_t *)(smem + kTableSmem) + gid * (32 * (TMAXN / (2 * G)) * (G / 32));
+  // digit counters nest like the slices: 1 KiB per warp, a group's counters
+  // start at its first warp's (a warp's radix needs 32 digits x 16 items x 2 B)
+  static_assert(32 * (TMAXN / (2 * G)) * (G / 32) * 2 <= (G / 32) * 1024, "counters");
+  static_assert((kThreads / 32) * 1024 <= kCountSmem, "counter space");
+  gm.cnt = (uint16_t *)(smem + kTableSmem + gid * (G / 32) * 1024);
   gm.tmp = sh.scan + slot * 33;
   gm.itmp = sh.itmp + slot * 18;
   gm.lst = sh.lst + gid * G;
   gm.nl = sh.nl + (G == 32 ? 12 + gid : slot);
   gm.cap = G;
+  // flat-loop staging: the free part of the slice above the largest table
+  static_assert(G == 32 || (NUM ? TMAXN * 12 : TMAXS * 4) + 24 * G <= SLICE, "staging");
+  gm.stage = G == 32 ? nullptr : slice + (NUM ? TMAXN * 12 : TMAXS * 4);
   const int64_t base = sh.off[cls], count = sh.cnt[cls];
   // rows are taken in chunks (one counter atomic per chunk); the chunk shrinks
   // to one row as the class runs out so the tail stays balanced
@@ -880,6 +977,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   gm.lst = sh.lst;
   gm.nl = sh.nl + 47;
   gm.cap = 1024;
+  gm.stage = nullptr;
   // stage 1: CTA-level rows, heaviest class first
   while (true) {
     if (tid == 0) sh.slot[15] = atomicAdd(&A.S->work, 1ull);
