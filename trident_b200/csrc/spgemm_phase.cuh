@@ -247,6 +247,14 @@ __device__ __forceinline__ void prof_add(const PhaseArgs &A, int cls, long long 
     atomicAdd(A.prof + NCLS + cls, 1ull);
   }
 }
+__device__ __forceinline__ void prof_sub_g(const PhaseArgs &A, int i, long long &t,
+                                           bool leader) {
+  if (A.prof && leader) {
+    const long long now = clock64();
+    atomicAdd(A.prof + kProfSub + i, (unsigned long long)(now - t));
+    t = now;
+  }
+}
 __device__ __forceinline__ void prof_sub(const PhaseArgs &A, int i, long long &t) {
   if (A.prof && threadIdx.x == 0) {
     const long long now = clock64();
@@ -286,6 +294,7 @@ template <int G, int TMAX, typename PT, typename VT>
 __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                              int64_t idx, int *keys, const GroupMem &gm, int gid,
                              int lane) {
+  long long tp = clock64();
   const RowRef rr = decode_row(A, idx);
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t f = A.rowf[rr.g];
@@ -298,6 +307,7 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  prof_sub_g(A, 9, tp, lane == 0);
   int cnt = 0;
   auto ins = [&](int32_t col, VT) { cnt += sym_insert(keys, col, logT, mask, A.err); };
   if constexpr (G <= 256) {
@@ -309,9 +319,11 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                                             gid, gm.lst, gm.nl, gm.cap, ins);
   }
   group_sync<G>(gid);
+  prof_sub_g(A, 10, tp, lane == 0);
   const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
   if (lane == 0) A.rowc[rr.g] = int32_t(total);
   group_sync<G>(gid);
+  prof_sub_g(A, 11, tp, lane == 0);
 }
 
 template <typename PT, typename VT>
@@ -376,17 +388,20 @@ __device__ __forceinline__ void bitonic_pairs(int *keys, VT *vals, uint32_t P,
   }
 }
 
-// Stable LSD radix sort of n <= ITEMS*G (key, value) pairs with 5-bit digits.
-// Element e sits at item e / G of thread e % G; within a warp, equal digits
-// are ranked with __match_any_sync.  cnt holds 32 digits x ITEMS x G/32
-// warps uint16 counters laid out (digit, item, warp), so one exclusive scan
-// over cnt yields every element's output base in stable order.  (ka, va) and
-// (kb, vb) alternate as source and destination; returns 1 when the sorted
-// pairs end in (kb, vb).
-template <int G, int ITEMS, typename VT>
+// Stable LSD radix sort of n <= ITEMS*G (key, value) pairs with RB-bit digits
+// (RAD * ITEMS = 512: fewer items per thread buy wider digits, so fewer
+// passes, in the same 1 KiB of counters per warp).  Element e sits at item
+// e / G of thread e % G; within a warp, equal digits are ranked with
+// __match_any_sync.  cnt holds RAD digits x ITEMS x G/32 warps uint16
+// counters laid out (digit, item, warp), so one exclusive scan over cnt
+// yields every element's output base in stable order.  (ka, va) and (kb, vb)
+// alternate as source and destination; returns 1 when the sorted pairs end in
+// (kb, vb).
+template <int G, int ITEMS, int RB, typename VT>
 __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
                            uint16_t *cnt, int64_t *tmp, int gid, int lane) {
-  constexpr int NW = G / 32, RB = 5, RAD = 1 << RB;
+  constexpr int NW = G / 32, RAD = 1 << RB;
+  static_assert(RAD * ITEMS == 512, "1 KiB of counters per warp");
   constexpr int E = RAD * ITEMS * NW, PER = E / G;
   static_assert(PER * G == E, "counter layout");
   const int w = lane >> 5;
@@ -402,12 +417,16 @@ __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
     int dig[ITEMS], rk[ITEMS];
 #pragma unroll
     for (int it = 0; it < ITEMS; ++it) {
-      const int e = it * G + lane;
-      const int d = e < n ? ((ks[e] >> shift) & (RAD - 1)) : RAD;
-      const unsigned m = __match_any_sync(0xffffffffu, d);
-      rk[it] = __popc(m & below);
-      dig[it] = d;
-      if (d < RAD && rk[it] == 0) cnt[(d * ITEMS + it) * NW + w] = uint16_t(__popc(m));
+      dig[it] = RAD;
+      rk[it] = 0;
+      if (it * G < n) {  // uniform across the group
+        const int e = it * G + lane;
+        const int d = e < n ? ((ks[e] >> shift) & (RAD - 1)) : RAD;
+        const unsigned m = __match_any_sync(0xffffffffu, d);
+        rk[it] = __popc(m & below);
+        dig[it] = d;
+        if (d < RAD && rk[it] == 0) cnt[(d * ITEMS + it) * NW + w] = uint16_t(__popc(m));
+      }
     }
     group_sync<G>(gid);
     int s = 0;
@@ -448,6 +467,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   static_assert(KEEP >= 1 && KEEP <= 16 && KEEP * 2 * G == TMAX, "compaction layout");
   VT *vals = (VT *)slice;
   int *keys = (int *)(slice + TMAX * 8);
+  long long tp = clock64();
   const RowRef rr = decode_row(A, idx);
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t c = A.rowc[rr.g];
@@ -462,6 +482,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
   group_sync<G>(gid);
   const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  prof_sub_g(A, 9, tp, lane == 0);
   auto ins = [&](int32_t col, VT v) {
     const uint32_t h = num_insert(keys, col, logT, mask, A.err);
     atomicAdd(vals + h, v);
@@ -476,6 +497,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                                            ins);
   }
   group_sync<G>(gid);
+  prof_sub_g(A, 10, tp, lane == 0);
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
   // so first-half slots are held in registers across the group barrier inside
   // group_minmax; second-half slots are never overwritten.
@@ -531,6 +553,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     }
   }
   group_sync<G>(gid);
+  prof_sub_g(A, 11, tp, lane == 0);
   int src = 0;
   if (!radix) {
     const uint32_t Pw = pow2_at_least(c, 2);
@@ -539,9 +562,18 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     bitonic_pairs<G, VT>(keys, vals, Pw, gid, lane);
   } else {
     const int bits = 32 - __clz(mx - mn);
-    src = radix_pairs<G, KEEP, VT>(keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid,
-                                   lane);
+    // widest digits whose item count still holds the row
+    if (KEEP >= 4 && c <= 4 * G)
+      src = radix_pairs<G, (KEEP < 4 ? KEEP : 4), (KEEP < 4 ? 5 : 7), VT>(
+          keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid, lane);
+    else if (KEEP >= 8 && c <= 8 * G)
+      src = radix_pairs<G, (KEEP < 8 ? KEEP : 8), (KEEP < 8 ? 5 : 6), VT>(
+          keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp, gid, lane);
+    else
+      src = radix_pairs<G, 16, 5, VT>(keys, vals, keys + H, vals + H, int(c), bits, cnt, tmp,
+                                      gid, lane);
   }
+  prof_sub_g(A, 12, tp, lane == 0);
   const int *ko = src ? keys + H : keys;
   const VT *vo = src ? vals + H : vals;
   int32_t *__restrict__ Cj = P.Cj + off;
@@ -551,6 +583,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     Cx[s] = vo[s];
   }
   group_sync<G>(gid);
+  prof_sub_g(A, 13, tp, lane == 0);
 }
 
 // DENSE numeric row, whole-row form (ncols <= kRankMaxCols).  Pass 1 sets the

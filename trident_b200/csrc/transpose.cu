@@ -47,7 +47,7 @@ __global__ void k_col_scatter(const PT *rp, const int32_t *col, const VT *val, i
 
 // One CTA per segment (grid-stride over segments): sort up to kSegCta pairs
 // of a segment (or one run of a longer segment) by key.
-constexpr int kSortSmem = 2 * kSegCta * 4 + 2 * kSegCta * 8 + 32 * 8 * (kSegThreads / 32) * 2;
+constexpr int kSortSmem = 2 * kSegCta * 4 + 2 * kSegCta * 8 + 64 * 8 * (kSegThreads / 32) * 2;
 
 template <typename VT>
 __global__ void __launch_bounds__(kSegThreads)
@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(kSegThreads)
       for (int i = tid; i < n; i += kSegThreads) ks[i] -= mn;
       __syncthreads();
       const int bits = mx > mn ? 32 - __clz(mx - mn) : 0;
-      const int src = radix_pairs<kSegThreads, 8, VT>(ks, vs, ks + kSegCta, vs + kSegCta, n, bits,
-                                                      cnt, tmp, 0, tid);
+      const int src = radix_pairs<kSegThreads, 8, 6, VT>(ks, vs, ks + kSegCta, vs + kSegCta, n,
+                                                         bits, cnt, tmp, 0, tid);
       const int *ko = src ? ks + kSegCta : ks;
       const VT *vo = src ? vs + kSegCta : vs;
       for (int i = tid; i < n; i += kSegThreads) {
