@@ -172,6 +172,8 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     A, cfg = make_workload(args)
     ctx = ops.Context(dev)
+    if args.workload == "rmat":
+        cfg["tuning"] = apply_tuning(ctx, "rmat")
     dA = A.to_device(rowptr_bits=32)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -406,6 +408,7 @@ def run_batched(args):
     torch.cuda.set_device(0)
     specs = workloads.batched_specs(args.products, seed=args.seed)
     ctx = ops.Context(0)
+    tuning = apply_tuning(ctx, "batched")
     dev, mults = [], 0
     for spec in specs:
         A, B = workloads.batched_product(spec)
@@ -464,7 +467,7 @@ def run_batched(args):
         "value": round(n / (ms * 1e-3), 1), "unit": "products/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poisson-row matrices, values U[-1,1])",
-        "config": {"workload": f"batched{n}", "products": n, "rows_total": int(sum(d[0].nrows for d in dev)),
+        "config": {"tuning": tuning, "workload": f"batched{n}", "products": n, "rows_total": int(sum(d[0].nrows for d in dev)),
                    "nnz_A_total": int(sum(d[0].nnz for d in dev)), "mults": int(mults),
                    "nnz_C_total": int(total_nnz), "rows": "log-uniform [1e3, 2e5]", "lambda": "U[8, 32]"},
         "gflops": round(2.0 * mults / (ms * 1e-3) / 1e9, 3),
@@ -492,6 +495,7 @@ def run_rap(args):
     torch.cuda.set_device(0)
     R, A, P = workloads.galerkin_operands(n=n, pts=27, agg=3)
     ctx = ops.Context(0)
+    tuning = apply_tuning(ctx, "rap")
     dR, dA, dP = R.to_device(), A.to_device(), P.to_device()
     m1 = ops.spgemm_count(ctx, dA, dP)[0]
     AP = ops.spgemm(ctx, dA, dP, rowptr_bits=32)
@@ -537,7 +541,7 @@ def run_rap(args):
         "metric": "Galerkin R·A·P GFLOP/s (2 x multiply-adds), FP64", "value": round(2.0 * (m1 + m2) / (ms * 1e-3) / 1e9, 3),
         "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": True, "dtype": "f64", "data": "synthetic (27-point Laplacian, SA prolongator)",
-        "config": {"workload": f"rap27pt_{n}^3", "nnz_A": A.nnz, "nnz_P": P.nnz, "nnz_AP": AP.nnz, "nnz_RAP": RAP.nnz,
+        "config": {"tuning": tuning, "workload": f"rap27pt_{n}^3", "nnz_A": A.nnz, "nnz_P": P.nnz, "nnz_AP": AP.nnz, "nnz_RAP": RAP.nnz,
                    "mults_AP": int(m1), "mults_RAP": int(m2)},
         "AP": {"ms": round(ap_ms, 3), "hbm_frac": round(bap / (ap_ms * 1e-3) / 1e9 / peak, 4)},
         "RAP": {"ms": round(ms - ap_ms, 3), "hbm_frac": round(brap / ((ms - ap_ms) * 1e-3) / 1e9 / peak, 4)},
@@ -562,6 +566,7 @@ def run_served(args):
     torch.cuda.set_device(0)
     rng = np.random.Generator(np.random.Philox(args.seed))
     ctx = ops.Context(0)
+    tuning = apply_tuning(ctx, "batched")
     ab_pool = []
     for spec in workloads.batched_specs(24, seed=args.seed + 1000):
         A, B = workloads.batched_product(spec)
@@ -629,7 +634,7 @@ def run_served(args):
         "metric": "served R·A·P + A·B req/s (Poisson arrivals), p50/p99 latency", "value": round(served, 1),
         "unit": "req/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic (resident pool: 24 A·B pairs, 8 R·A·P sets)",
-        "config": {"workload": "served", "rate": args.rate, "duration_s": args.duration, "requests": n_req,
+        "config": {"tuning": tuning, "workload": "served", "rate": args.rate, "duration_s": args.duration, "requests": n_req,
                    "ab_share": 0.7, "budget_gb": 120, "lanes": 3, "max_batch": 64},
         "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
         "batches": stats["batches"], "loop_of_plain_calls": {"req_per_s": round(n_req / loop_s, 1)},
@@ -637,6 +642,18 @@ def run_served(args):
     }
     ctx.close()
     return line
+
+
+def apply_tuning(ctx, name):
+    """Apply the committed autotuner file of a workload (trident_b200/tuning/
+    <name>.json, written by `python -m trident_b200.tune`), if there is one;
+    returns what goes into the JSON line's config."""
+    from trident_b200 import tune
+    path = tune.tuning_path(name)
+    if not os.path.exists(path):
+        return None
+    t = ctx.load_tuning(path)
+    return {"file": os.path.relpath(path, os.path.dirname(os.path.abspath(__file__))), **t}
 
 
 def main():

@@ -134,12 +134,33 @@ int tspg_ctx_mem(const tspg_ctx *ctx, size_t *in_use, size_t *high_water);
 int tspg_ctx_stats(const tspg_ctx *ctx, int64_t *launches);
 int tspg_ctx_phase_timing(tspg_ctx *ctx, int enable);
 int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
+/* Row binning of the SpGEMM (no counterpart in the reference, whose binning
+ * lives inside KokkosKernels / cuSPARSE): rows go to warp / 128-thread /
+ * 256-thread / CTA groups by the upper bounds sym_lim[] (symbolic phase, on
+ * min(products, ncols)) and num_lim[] (numeric phase, on the row's nnz); rows
+ * above the last bound are DENSE rows.  hash_load = hash-table slots per key
+ * (2, 4 or 8).  Bounds must be positive, non-decreasing and at most the table
+ * capacities sym <= {512, 2048, 4096, 24576}, num <= {512, 1024, 2048, 8192}
+ * (the defaults); otherwise TSPG_EINVAL.  Applies to calls made after it;
+ * results do not depend on it. */
+typedef struct tspg_tuning {
+  int32_t sym_lim[4];
+  int32_t num_lim[4];
+  int32_t hash_load;
+  int32_t reserved[3];
+} tspg_tuning;
+int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t);
+int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t);
+
 /* Per-class accounting of the persistent phases (off by default): SM cycles
  * and rows per row class, accumulated over calls since enabling.  out64 =
  * symbolic[32], numeric[32]; each half holds cycles x 7, rows x 7 (classes
  * DENSE0 (>= 2^20 products), DENSE1 (>= 2^17), DENSE2, G1024, G256, G128,
- * G32), then (numeric only) cycles of the whole-row DENSE rows' bitmap
- * pass, column scan and value pass.  Reading synchronises the
+ * G32), then sub-phase cycles: [14..18] the whole-row DENSE rows' bitmap
+ * pass, block scan, zero fill, column emission and value pass; [19..22] the
+ * windowed DENSE rows' set-up, short-entry walks, long-entry walks and
+ * emission; [23..27] the group rows' set-up, products, compaction, sort and
+ * write (symbolic: set-up, products, count).  Reading synchronises the
  * device. */
 int tspg_ctx_class_profile(tspg_ctx *ctx, int enable);
 int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out64);
@@ -297,7 +318,8 @@ typedef struct tspg_server_config {
   int lanes;         /* concurrent worker lanes (1..16) */
   int max_batch;     /* requests per batch */
 } tspg_server_config;
-/* The server uses ctx's device; it creates its own contexts and streams. */
+/* The server uses ctx's device; it creates its own contexts and streams,
+ * which take ctx's row binning (tspg_ctx_set_tuning) at creation. */
 int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
                        tspg_server **out);
 int tspg_server_destroy(tspg_server *s);

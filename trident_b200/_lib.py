@@ -50,6 +50,16 @@ class TspgCsrOut(C.Structure):
     ]
 
 
+class TspgTuning(C.Structure):
+    """Row binning (tspg_tuning): group-class bounds and hash slots per key."""
+    _fields_ = [
+        ("sym_lim", C.c_int32 * 4),
+        ("num_lim", C.c_int32 * 4),
+        ("hash_load", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+
 class TspgServerConfig(C.Structure):
     _fields_ = [("mem_budget", C.c_size_t), ("lanes", C.c_int), ("max_batch", C.c_int)]
 
@@ -92,6 +102,8 @@ def _load() -> C.CDLL:
         "tspg_ctx_stats": (i32, [vp, P(i64)]),
         "tspg_ctx_phase_timing": (i32, [vp, i32]),
         "tspg_ctx_phase_ms": (i32, [vp, P(C.c_float), P(C.c_float)]),
+        "tspg_ctx_set_tuning": (i32, [vp, P(TspgTuning)]),
+        "tspg_ctx_get_tuning": (i32, [vp, P(TspgTuning)]),
         "tspg_ctx_class_profile": (i32, [vp, i32]),
         "tspg_ctx_class_cycles": (i32, [vp, P(C.c_uint64)]),
         "tspg_batch_create": (i32, [vp, P(vp)]),

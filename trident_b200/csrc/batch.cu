@@ -14,6 +14,7 @@
 //   graph 2: output pointers, numeric binning, numeric k_phase.
 // The graphs are captured on the first run and replayed while the batch's
 // operands are unchanged; tspg_batch_add / clear drop them.
+#include <cstring>
 #include <new>
 #include <vector>
 
@@ -82,6 +83,7 @@ struct tspg_batch {
   int32_t *rowc = nullptr;
   uint64_t *list = nullptr;
   Sched *sched = nullptr;
+  Tune tune{};  // row binning the graphs were captured with
   int32_t *curbuf = nullptr;
   int64_t cur_stride = 0;
   int32_t *Cj = nullptr;
@@ -165,7 +167,10 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_phase<PT, VT, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
-  const bool rebuild = b->dirty || !b->g1 || b->gstream != s;
+  // the graphs hold the row binning of their capture: a new tuning re-captures
+  const bool retune = std::memcmp(&b->tune, &ctx->tune, sizeof(Tune)) != 0;
+  const bool rebuild = b->dirty || !b->g1 || b->gstream != s || retune;
+  b->tune = ctx->tune;
   if (rebuild) {
     b->drop_graphs();
     // layout
@@ -262,6 +267,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
     cudaGraph_t g;
     TSPG_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->sched, 0, 2 * sizeof(Sched), s);
+    k_set_tune<<<1, 32, 0, s>>>(b->sched, 2, ctx->tune);
     cudaMemsetAsync(b->rowc, 0, sizeof(int32_t) * (R > 0 ? R : 1), s);
     cudaMemsetAsync(b->cp, 0, sizeof(int64_t), s);
     if (!(flags & TSPG_F_B_SORTED) && b->RB > 0)
@@ -286,7 +292,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                                          b->sched + 1, b->rowf);
     }
     k_gather_offsets<<<(nprod + 256) / 256, 256, 0, s>>>(b->cp, b->d_base, nprod, b->offs);
-    b->g1_kernels = 1 + (!(flags & TSPG_F_B_SORTED) && b->RB > 0) + (R > 0 ? 7 : 0);
+    b->g1_kernels = 2 + (!(flags & TSPG_F_B_SORTED) && b->RB > 0) + (R > 0 ? 7 : 0);
     cudaMemcpyAsync(b->h_offs, b->offs, sizeof(int64_t) * (nprod + 1), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(b->h_offs + nprod + 1, &b->sched[0].max_a_row, sizeof(int64_t),
                     cudaMemcpyDeviceToHost, s);

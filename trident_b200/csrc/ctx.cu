@@ -174,6 +174,30 @@ extern "C" int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms,
   return TSPG_OK;
 }
 
+extern "C" int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t) {
+  if (!ctx || !t) return TSPG_EINVAL;
+  Tune u{};
+  for (int i = 0; i < 4; ++i) {
+    u.sym[i] = t->sym_lim[i];
+    u.num[i] = t->num_lim[i];
+  }
+  u.load = t->hash_load;
+  if (!tune_valid(u)) return TSPG_EINVAL;
+  ctx->tune = u;
+  return TSPG_OK;
+}
+
+extern "C" int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t) {
+  if (!ctx || !t) return TSPG_EINVAL;
+  for (int i = 0; i < 4; ++i) {
+    t->sym_lim[i] = ctx->tune.sym[i];
+    t->num_lim[i] = ctx->tune.num[i];
+  }
+  t->hash_load = ctx->tune.load;
+  t->reserved[0] = t->reserved[1] = t->reserved[2] = 0;
+  return TSPG_OK;
+}
+
 extern "C" int tspg_ctx_class_profile(tspg_ctx *ctx, int enable) {
   if (!ctx) return TSPG_EINVAL;
   TSPG_CUDA(ctx, cudaSetDevice(ctx->device));

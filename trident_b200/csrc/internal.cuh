@@ -11,6 +11,39 @@
 
 #include "tspg.h"
 
+namespace tspg {
+// Class limits = table capacities (symbolic: on min(mults, ncols); numeric: on
+// the row's nnz).  Symbolic tables hold int32 keys (128 KiB per CTA), numeric
+// tables hold key + FP64 value (192 KiB per CTA); a table has T = pow2 >=
+// load x the bound slots.
+constexpr int64_t kSymLim32 = 512, kSymLim128 = 2048, kSymLim256 = 4096, kSymLim1024 = 24576;
+constexpr int64_t kNumLim32 = 512, kNumLim128 = 1024, kNumLim256 = 2048, kNumLim1024 = 8192;
+
+// Runtime row-binning parameters (the autotuned part of the SpGEMM): upper
+// bounds of the warp / 128 / 256 / CTA group classes, symbolic on
+// min(products, ncols) and numeric on the row's nnz, and the hash-table slots
+// per key.  Bounds never exceed the compile-time table capacities
+// (kSymLim*, kNumLim*); tspg_ctx_set_tuning checks that.
+struct Tune {
+  int32_t sym[4];
+  int32_t num[4];
+  int32_t load;
+  int32_t pad[3];
+};
+
+// A tuning is valid when every bound is positive, non-decreasing over the
+// classes and within the table capacity of its class, and load is 2, 4 or 8.
+inline bool tune_valid(const Tune &t) {
+  const int64_t smax[4] = {kSymLim32, kSymLim128, kSymLim256, kSymLim1024};
+  const int64_t nmax[4] = {kNumLim32, kNumLim128, kNumLim256, kNumLim1024};
+  for (int i = 0; i < 4; ++i) {
+    if (t.sym[i] < 1 || t.sym[i] > smax[i] || t.num[i] < 1 || t.num[i] > nmax[i]) return false;
+    if (i > 0 && (t.sym[i] < t.sym[i - 1] || t.num[i] < t.num[i - 1])) return false;
+  }
+  return t.load == 2 || t.load == 4 || t.load == 8;
+}
+}  // namespace tspg
+
 struct tspg_ctx {
   int device = 0;
   int num_sms = 0;
@@ -33,6 +66,13 @@ struct tspg_ctx {
   bool ev_sym = false, ev_num = false;
   // per-class cycle accounting of the persistent phases: [phase][2 * 7]
   unsigned long long *d_prof = nullptr;
+  // row binning (tspg_ctx_set_tuning); the defaults are the table capacities
+  tspg::Tune tune = {{int32_t(tspg::kSymLim32), int32_t(tspg::kSymLim128),
+                      int32_t(tspg::kSymLim256), int32_t(tspg::kSymLim1024)},
+                     {int32_t(tspg::kNumLim32), int32_t(tspg::kNumLim128),
+                      int32_t(tspg::kNumLim256), int32_t(tspg::kNumLim1024)},
+                     2,
+                     {0, 0, 0}};
 };
 
 namespace tspg {

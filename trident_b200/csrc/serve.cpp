@@ -212,10 +212,13 @@ extern "C" int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
   int st = tspg_ctx_create(dev, 0, &S->adm);
   if (st == TSPG_OK && cudaStreamCreateWithFlags(&S->adm_stream, cudaStreamNonBlocking) != cudaSuccess)
     st = TSPG_ECUDA;
+  tspg_tuning tune;  // lanes take the row binning of the parent context
+  if (st == TSPG_OK) st = tspg_ctx_get_tuning(ctx, &tune);
   for (int l = 0; l < cfg->lanes && st == TSPG_OK; ++l) {
     tspg_ctx *c = nullptr;
     cudaStream_t ls = nullptr;
     st = tspg_ctx_create(dev, 0, &c);
+    if (st == TSPG_OK) st = tspg_ctx_set_tuning(c, &tune);
     if (st == TSPG_OK && cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking) != cudaSuccess)
       st = TSPG_ECUDA;
     S->lane_ctx.push_back(c);

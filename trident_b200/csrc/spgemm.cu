@@ -106,6 +106,7 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   TSPG_TRY(P->get(&P->sched, 2));
   TSPG_TRY(P->get(&P->partial, P->nb + 1));
   TSPG_CUDA(ctx, cudaMemsetAsync(P->sched, 0, 2 * sizeof(Sched), s));
+  k_set_tune<<<1, 32, 0, s>>>(P->sched, 2, ctx->tune);
   TSPG_CUDA(ctx, cudaMemsetAsync(P->rowc, 0, (m > 0 ? m : 1) * sizeof(int32_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(P->cp, 0, sizeof(int64_t), s));
 
@@ -142,7 +143,7 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                                                           P->nb, P->cp, P->sched + 1, P->rowf);
   }
   TSPG_CUDA(ctx, cudaGetLastError());
-  ctx->launches += 1 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 7 : 0);
+  ctx->launches += 2 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 7 : 0);
   int64_t *h = ctx->h_words;
   TSPG_CUDA(ctx, cudaMemcpyAsync(h, P->cp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   TSPG_CUDA(ctx, cudaMemcpyAsync(h + 1, &P->sched[0].total, 4 * sizeof(int64_t),
@@ -392,6 +393,7 @@ extern "C" int tspg_spgemm_count(tspg_ctx *ctx, void *stream,
     TSPG_TRY(sc.get(&rowf, m));
     TSPG_TRY(sc.get(&sched, 1));
     TSPG_CUDA(ctx, cudaMemsetAsync(sched, 0, sizeof(Sched), s));
+    k_set_tune<<<1, 32, 0, s>>>(sched, 1, ctx->tune);
     ProdDev<PT, VT> v{};
     v.Ap = (const PT *)A->rowptr;
     v.Aj = A->col;
@@ -402,7 +404,7 @@ extern "C" int tspg_spgemm_count(tspg_ctx *ctx, void *stream,
     if (m > 0)
       k_row_mults<PT, VT><<<grid_for(m * 32, 256, ctx->num_sms * 16), 256, 0, s>>>(
           prods, base, 1, m, rowf, sched);
-    ctx->launches += 1 + (m > 0);
+    ctx->launches += 2 + (m > 0);
     TSPG_CUDA(ctx, cudaGetLastError());
     int64_t *h = ctx->h_words;
     TSPG_CUDA(ctx, cudaMemcpyAsync(h, &sched->total, 2 * sizeof(int64_t),

@@ -52,13 +52,6 @@ enum {
 constexpr int kCtaClasses = 4;  // classes [0, 4) are CTA-level
 __host__ __device__ constexpr bool cls_dense(int c) { return c <= CLS_DENSE2; }
 
-// Class limits (symbolic: on min(mults, ncols); numeric: on the row's nnz).
-// Symbolic tables hold int32 keys (128 KiB per CTA), numeric tables hold
-// key + FP64 value (192 KiB per CTA); a table has T = pow2 >= 2x the bound.
-__host__ __device__ constexpr int64_t kSymLim32 = 512, kSymLim128 = 2048,
-                                      kSymLim256 = 4096, kSymLim1024 = 24576;
-__host__ __device__ constexpr int64_t kNumLim32 = 512, kNumLim128 = 1024,
-                                      kNumLim256 = 2048, kNumLim1024 = 8192;
 constexpr int kSymT32 = 1024, kSymT128 = 4096, kSymT256 = 8192,
               kSymT1024 = 32768;
 constexpr int kNumT32 = 1024, kNumT128 = 2048, kNumT256 = 4096,
@@ -74,23 +67,24 @@ constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 196) * 1024;
 __host__ __device__ inline int dense_sub(int64_t f) {
   return f >= (int64_t(1) << 20) ? CLS_DENSE0 : f >= (int64_t(1) << 17) ? CLS_DENSE1 : CLS_DENSE2;
 }
-__host__ __device__ inline int sym_class(int64_t f, int64_t n) {
+__host__ __device__ inline int sym_class(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
   if (f == 0) return -1;
-  if (fe <= kSymLim32) return CLS_G32;
-  if (fe <= kSymLim128) return CLS_G128;
-  if (fe <= kSymLim256) return CLS_G256;
-  if (fe <= kSymLim1024) return CLS_G1024;
+  if (fe <= t.sym[0]) return CLS_G32;
+  if (fe <= t.sym[1]) return CLS_G128;
+  if (fe <= t.sym[2]) return CLS_G256;
+  if (fe <= t.sym[3]) return CLS_G1024;
   return dense_sub(f);
 }
-__host__ __device__ inline int num_class(int64_t c, int64_t f) {
+__host__ __device__ inline int num_class(int64_t c, int64_t f, const Tune &t) {
   if (c == 0) return -1;
-  if (c <= kNumLim32) return CLS_G32;
-  if (c <= kNumLim128) return CLS_G128;
-  if (c <= kNumLim256) return CLS_G256;
-  if (c <= kNumLim1024) return CLS_G1024;
+  if (c <= t.num[0]) return CLS_G32;
+  if (c <= t.num[1]) return CLS_G128;
+  if (c <= t.num[2]) return CLS_G256;
+  if (c <= t.num[3]) return CLS_G1024;
   return dense_sub(f);
 }
+
 
 template <typename PT, typename VT>
 struct ProdDev {
@@ -111,6 +105,7 @@ struct ProdDev {
 // Work schedule of one phase: rows per class, their list offsets and the
 // work-item prefix the persistent kernel decodes.
 struct Sched {
+  Tune tune;  // row binning of this run, set by k_set_tune after the reset
   int64_t cnt[NCLS];
   int64_t off[NCLS];
   int64_t cur[NCLS];
@@ -167,6 +162,11 @@ __device__ __forceinline__ int subgroup_width_avg(int64_t f, int64_t na, int G) 
 
 // ---------------------------------------------------------------------------
 // Setup kernels
+
+// Row binning of a run into its Sched records (after they were zeroed).
+static __global__ void k_set_tune(Sched *S, int n, Tune t) {
+  if (threadIdx.x < n) S[threadIdx.x].tune = t;
+}
 
 template <typename PT, typename VT>
 __global__ void k_set_prod(ProdDev<PT, VT> *dst, ProdDev<PT, VT> v,
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_row_mults(
     if (lane == 0) {
       rowf[g] = f;
       const int64_t n = prods[p].n;
-      const int c = sym_class(f, n);
+      const int c = sym_class(f, n, S->tune);
       if (c >= 0) {
         atomicAdd(&s_cnt[c], 1ull);
         ne += 1;
@@ -311,9 +311,9 @@ __global__ void __launch_bounds__(256) k_scatter(
     p = find_prod(base, nprod, g);
     r = g - base[p];
     if (MODE == 0) {
-      c = sym_class(rowf[g], prods[p].n);
+      c = sym_class(rowf[g], prods[p].n, S->tune);
     } else {
-      c = num_class(rowc[g], rowf[g]);
+      c = num_class(rowc[g], rowf[g], S->tune);
       const int64_t off = cp[g] - cp[base[p]];
       if (prods[p].cp_bits == 32)
         ((int32_t *)prods[p].Cp)[r] = (int32_t)off;
@@ -414,7 +414,7 @@ static __global__ void __launch_bounds__(kScanThreads)
   for (int i = 0; i < kScanItems; ++i) {
     v[i] = (j0 + i < R) ? in[j0 + i] : 0;
     s += v[i];
-    if (rowf && v[i] > 0) atomicAdd(&s_cnt[num_class(v[i], rowf[j0 + i])], 1ull);
+    if (rowf && v[i] > 0) atomicAdd(&s_cnt[num_class(v[i], rowf[j0 + i], Snum->tune)], 1ull);
   }
   int64_t tot;
   int64_t ex = group_excl_scan<kScanThreads, int64_t>(s, tmp, 0, &tot);

@@ -300,7 +300,7 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const int64_t f = A.rowf[rr.g];
   const int64_t n = P.n;
   const int64_t fe = f < n ? f : n;
-  uint32_t T = pow2_at_least(2 * fe, 32);
+  uint32_t T = pow2_at_least(A.S->tune.load * fe, 32);
   if (T > TMAX) T = TMAX;
   const int logT = ilog2_pow2(T);
   const uint32_t mask = T - 1;
@@ -472,7 +472,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   const ProdDev<PT, VT> &P = prods[rr.p];
   const int64_t c = A.rowc[rr.g];
   const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
-  uint32_t T = pow2_at_least(2 * c, 32);
+  uint32_t T = pow2_at_least(A.S->tune.load * c, 32);
   if (T > TMAX) T = TMAX;
   const int logT = ilog2_pow2(T);
   const uint32_t mask = T - 1;

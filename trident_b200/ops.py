@@ -13,7 +13,7 @@ import ctypes as C
 
 import torch
 
-from ._lib import (ALLOC_FN, TSPG_COLS, TSPG_ENOMEM, TSPG_OK, TSPG_ROWS, TspgCsr,
+from ._lib import (ALLOC_FN, TSPG_COLS, TSPG_ENOMEM, TSPG_OK, TSPG_ROWS, TspgCsr, TspgTuning,
                    TspgCsrOut, TspgError, check, lib)
 from .csr import DeviceCSR
 
@@ -62,6 +62,33 @@ class Context:
         a, b = C.c_size_t(), C.c_size_t()
         check(lib.tspg_ctx_mem(self.h, C.byref(a), C.byref(b)), "tspg_ctx_mem")
         return a.value, b.value
+
+    def get_tuning(self) -> dict:
+        """Row binning in force: {"sym_lim": [4], "num_lim": [4], "hash_load": k}."""
+        t = TspgTuning()
+        check(lib.tspg_ctx_get_tuning(self.h, C.byref(t)), "tspg_ctx_get_tuning")
+        return {"sym_lim": list(t.sym_lim), "num_lim": list(t.num_lim), "hash_load": t.hash_load}
+
+    def set_tuning(self, tuning: dict):
+        """Set the row binning (keys as get_tuning returns; missing keys keep
+        their current values).  Raises TspgError(TSPG_EINVAL) when a bound is
+        out of range."""
+        cur = self.get_tuning()
+        cur.update({k: tuning[k] for k in ("sym_lim", "num_lim", "hash_load") if k in tuning})
+        t = TspgTuning()
+        for i in range(4):
+            t.sym_lim[i] = int(cur["sym_lim"][i])
+            t.num_lim[i] = int(cur["num_lim"][i])
+        t.hash_load = int(cur["hash_load"])
+        check(lib.tspg_ctx_set_tuning(self.h, C.byref(t)), "tspg_ctx_set_tuning")
+
+    def load_tuning(self, path: str) -> dict:
+        """Apply the "tuning" object of an autotuner JSON file; returns it."""
+        import json
+        with open(path) as fh:
+            doc = json.load(fh)
+        self.set_tuning(doc["tuning"])
+        return doc["tuning"]
 
 
 def _out_struct(nrows, ncols, rowptr, val_bits, col=None, val=None, capacity=0, alloc=None):
