@@ -44,7 +44,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="rmat", choices=["rmat", "uniform", "batched", "rap", "served"])
+    p.add_argument("--workload", default="rmat",
+                   choices=["rmat", "uniform", "batched", "rap", "served", "summa"])
     p.add_argument("--rate", type=float, default=2000.0)
     p.add_argument("--duration", type=float, default=5.0)
     p.add_argument("--products", type=int, default=512)
@@ -247,6 +248,7 @@ def run_ours(args, rank, world):
     except Exception:
         peak, peak_src = 6650.0, "fallback"
     achieved = algo / (dom_ms * 1e-3) / 1e9
+    gather = algo + 8 * A.nnz + 12 * mults
     traffic = None
     try:
         prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
@@ -276,7 +278,10 @@ def run_ours(args, rank, world):
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic, "algorithmic_bytes": algo,
-                     "step_frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4)},
+                     "step_frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4),
+                     # Gustavson gather model: + B row offsets per A entry + B row contents per product
+                     "gather_model_bytes": gather,
+                     "gather_frac": round(gather / (dom_ms * 1e-3) / 1e9 / peak, 4)},
         "gpu_launches": int(launches1.value - launches0.value),
         "clocks": clk,
         "e2e": e2e,
@@ -644,6 +649,54 @@ def run_served(args):
     return line
 
 
+def run_summa(args):
+    """R-MAT A·A as a 4 x 4 tile grid with bitmask-compressed tiles, the four
+    SUMMA stages in sequence on one GPU (per stage and output tile: masks,
+    pack / unpack of A(i,q) and B(q,j), C(i,j) += A'·B').  Scale --scale
+    (default 19 here: the tiles, the stage partials and their merges of scale
+    20 need more than the GPU's memory at once); one step = the whole SUMMA."""
+    import torch
+
+    from trident_b200 import ops, summa, workloads
+    scale = args.scale if args.scale != 20 else 19
+    torch.cuda.set_device(0)
+    A = workloads.rmat(scale=scale, edge_factor=args.edge_factor, seed=args.seed)
+    ctx = ops.Context(0)
+    tuning = apply_tuning(ctx, "rmat")
+    q = 4
+    tiles, rb, cb = summa.cut_tiles(A, q)
+    dT = [[tiles[i][j].to_device() for j in range(q)] for i in range(q)]
+    mults = ops.spgemm_count(ctx, A.to_device(), A.to_device())[0]
+    stats = summa.StageStats()
+    C = summa.summa(ctx, dT, dT, q, use_masks=True, stats=stats)  # warm-up, sizes
+    nnz_c = sum(C[i][j].nnz for i in range(q) for j in range(q))
+    del C
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(max(1, args.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        C = summa.summa(ctx, dT, dT, q, use_masks=True)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        del C
+    ms = sorted(times)[len(times) // 2]
+    line = {
+        "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64, 4x4 SUMMA with bitmask-compressed tiles",
+        "value": round(2.0 * mults / (ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s", "n_gpus": 1,
+        "steps": len(times), "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded R-MAT, values U[-1,1])",
+        "config": {"tuning": tuning, "workload": f"rmat{scale}_summa4x4", "rows": A.nrows, "nnz_A": A.nnz,
+                   "mults": int(mults), "nnz_C": int(nnz_c), "grid": "4x4 tiles, 4 stages x 16 products"},
+        "tiles": {"a_nnz": stats.a_nnz, "a_kept": stats.a_kept, "b_nnz": stats.b_nnz,
+                  "b_kept": stats.b_kept, "packed_bytes": stats.packed_bytes,
+                  "full_bytes": stats.full_bytes},
+    }
+    ctx.close()
+    return line
+
+
 def apply_tuning(ctx, name):
     """Apply the committed autotuner file of a workload (trident_b200/tuning/
     <name>.json, written by `python -m trident_b200.tune`), if there is one;
@@ -658,8 +711,9 @@ def apply_tuning(ctx, name):
 
 def main():
     args = parse()
-    if args.impl == "ours" and args.workload in ("batched", "rap", "served"):
-        fn = {"batched": run_batched, "rap": run_rap, "served": run_served}[args.workload]
+    if args.impl == "ours" and args.workload in ("batched", "rap", "served", "summa"):
+        fn = {"batched": run_batched, "rap": run_rap, "served": run_served,
+              "summa": run_summa}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
     rank = int(os.environ.get("RANK", 0))
