@@ -41,6 +41,30 @@ def test_spadd_long_rows(ctx):
     check_sum(ops.spadd(ctx, A.to_device(), B.to_device()), A, B)
 
 
+def test_spadd_heavy_and_light_rows(ctx):
+    # rows merged by a CTA (above 4096 entries together) next to warp rows:
+    # full overlap, one side empty, disjoint interleaved, partial overlap
+    n = 50000
+    rng = np.random.default_rng(6)
+    light = random_csr(300, n, density=0.0005, seed=7)
+    lightB = random_csr(300, n, density=0.0005, seed=8)
+    full = np.sort(rng.choice(n, 10000, replace=False))
+    rowsA = [full, np.sort(rng.choice(n, 5000, replace=False)), np.zeros(0, np.int64),
+             np.arange(0, 12000, 2), np.sort(rng.choice(n, 3000, replace=False))]
+    rowsB = [full, np.zeros(0, np.int64), np.sort(rng.choice(n, 8000, replace=False)),
+             np.arange(1, 12000, 2), np.sort(rng.choice(n, 3000, replace=False))]
+
+    def build(heavy_rows, L):
+        rows = heavy_rows + [L.col[L.rowptr[i]:L.rowptr[i + 1]] for i in range(L.nrows)]
+        rp = np.zeros(len(rows) + 1, dtype=np.int64)
+        rp[1:] = np.cumsum([len(r) for r in rows])
+        col = np.concatenate(rows).astype(np.int32)
+        return HostCSR(len(rows), n, rp, col, rng.uniform(-1, 1, col.size))
+    A, B = build(rowsA, light), build(rowsB, lightB)
+    check_sum(ops.spadd(ctx, A.to_device(), B.to_device()), A, B)
+    check_sum(ops.spadd(ctx, B.to_device(rowptr_bits=32), A.to_device()), B, A)
+
+
 def test_sp_mma_accumulates_stages(ctx):
     # C = sum_q A_q B_q over 3 stages, as a SUMMA stage loop does
     As = [random_csr(400, 300, density=0.02, seed=20 + q) for q in range(3)]

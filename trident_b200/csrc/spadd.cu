@@ -6,8 +6,13 @@
 // numeric).  Rows are sorted and duplicate-free, so every entry finds its
 // output slot independently: an A entry at row position i lands at
 // i + |{b in B row : b < a}|, a B entry that is not in A at
-// j + |{a in A row : a < b}|.  One warp per row; lanes take entries and binary
-// search the other row (which sits in L1 after the first probes).
+// j + |{a in A row : a < b}|.  Rows with up to kMergeHeavy entries in A and B
+// together: one warp per row; lanes take entries and binary search the other
+// row (which sits in L1 after the first probes).  Longer rows (the hub rows of
+// partial C tiles reach 10^5 entries, and one warp per such row left the merge
+// waiting on a handful of warps) are listed and merged by a whole CTA along a
+// merge path: thread t takes steps [t, t+1) x (|A|+|B|) / threads of the
+// merged sequence (A before B on equal columns).
 #include "internal.cuh"
 #include "spgemm_kernels.cuh"
 
@@ -23,15 +28,22 @@ __device__ __forceinline__ int64_t lower_bound_row(const int32_t *col, int64_t l
   return lo;
 }
 
+constexpr int64_t kMergeHeavy = 4096;  // rows above this go to the CTA merge
+constexpr int kMergeThreads = 512;
+
 template <typename PTA, typename PTB>
 __global__ void __launch_bounds__(256)
     k_spadd_count(int64_t m, const PTA *Ap, const int32_t *Aj, const PTB *Bp,
-                  const int32_t *Bj, int32_t *rowc) {
+                  const int32_t *Bj, int32_t *rowc, int64_t *heavy, int64_t *nheavy) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t r = warp; r < m; r += nwarps) {
     const int64_t a0 = Ap[r], a1 = Ap[r + 1], b0 = Bp[r], b1 = Bp[r + 1];
+    if ((a1 - a0) + (b1 - b0) > kMergeHeavy) {
+      if (lane == 0) heavy[atomicAdd((unsigned long long *)nheavy, 1ull)] = r;
+      continue;
+    }
     int dup = 0;
     if (b1 > b0) {
       for (int64_t p = a0 + lane; p < a1; p += 32) {
@@ -72,6 +84,7 @@ __global__ void __launch_bounds__(256)
         else ((int64_t *)Cp)[m] = cp[m];
       }
     }
+    if ((a1 - a0) + (b1 - b0) > kMergeHeavy) continue;  // merged by k_spadd_heavy
     int running = 0;
     for (int64_t base = a0; base < a1; base += 32) {
       const int64_t p = base + lane;
@@ -109,13 +122,93 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Merge path of one heavy row inside a CTA.  Thread t covers the merged
+// steps [d0, d1); an A entry equal to the B entry at the B cursor takes that
+// B value too (it may lie past the thread's range), and a B entry equal to the
+// A entry before it is skipped, so a column present in both rows is emitted
+// once whichever thread holds either half.  WRITE = false counts the row's
+// union size; WRITE = true writes the row at (cj, cx).
+template <bool WRITE, typename VT>
+__device__ int64_t merge_row_cta(const int32_t *__restrict__ aj, const VT *__restrict__ ax,
+                                 int64_t la, const int32_t *__restrict__ bj,
+                                 const VT *__restrict__ bx, int64_t lb, int64_t *tmp,
+                                 int32_t *cj, VT *cx) {
+  const int tid = threadIdx.x;
+  const int64_t tot = la + lb;
+  const int64_t d0 = tot * tid / kMergeThreads, d1 = tot * (tid + 1) / kMergeThreads;
+  // largest i with A[i-1] <= B[d0-i]: the A entries among the first d0 steps
+  int64_t lo = d0 > lb ? d0 - lb : 0, hi = d0 < la ? d0 : la;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(aj + mid - 1) <= __ldg(bj + d0 - mid)) lo = mid; else hi = mid - 1;
+  }
+  int64_t i = lo, j = d0 - lo;
+  auto step = [&](bool emit, int64_t pos) -> int {  // 1 if the step makes an output
+    const bool take_a = i < la && (j >= lb || __ldg(aj + i) <= __ldg(bj + j));
+    if (take_a) {
+      if (emit) {
+        const int32_t x = __ldg(aj + i);
+        VT v = __ldg(ax + i);
+        if (j < lb && __ldg(bj + j) == x) v += __ldg(bx + j);
+        cj[pos] = x;
+        cx[pos] = v;
+      }
+      ++i;
+      return 1;
+    }
+    const int32_t x = __ldg(bj + j);
+    const bool dup = i > 0 && __ldg(aj + i - 1) == x;
+    if (emit && !dup) {
+      cj[pos] = x;
+      cx[pos] = __ldg(bx + j);
+    }
+    ++j;
+    return dup ? 0 : 1;
+  };
+  const int64_t si = i, sj = j;
+  int64_t n = 0;
+  for (int64_t d = d0; d < d1; ++d) n += step(false, 0);
+  int64_t all;
+  const int64_t base = group_excl_scan<kMergeThreads, int64_t>(n, tmp, 0, &all);
+  if constexpr (WRITE) {
+    i = si;
+    j = sj;
+    int64_t pos = base;
+    for (int64_t d = d0; d < d1; ++d) pos += step(true, pos);
+  }
+  return all;
+}
+
+// The listed heavy rows, one CTA each (persistent over the list).
+template <bool WRITE, typename PTA, typename PTB, typename VT>
+__global__ void __launch_bounds__(kMergeThreads)
+    k_spadd_heavy(const int64_t *heavy, const int64_t *nheavy, const PTA *Ap,
+                  const int32_t *Aj, const VT *Ax, const PTB *Bp, const int32_t *Bj,
+                  const VT *Bx, int32_t *rowc, const int64_t *cp, int32_t *Cj, VT *Cx) {
+  __shared__ int64_t tmp[kMergeThreads / 32 + 1];
+  const int64_t nh = *nheavy;
+  for (int64_t h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int64_t r = heavy[h];
+    const int64_t a0 = Ap[r], a1 = Ap[r + 1], b0 = Bp[r], b1 = Bp[r + 1];
+    if constexpr (WRITE) {
+      merge_row_cta<true, VT>(Aj + a0, Ax + a0, a1 - a0, Bj + b0, Bx + b0, b1 - b0, tmp,
+                              Cj + cp[r], Cx + cp[r]);
+    } else {
+      const int64_t n = merge_row_cta<false, VT>(Aj + a0, nullptr, a1 - a0, Bj + b0, nullptr,
+                                                 b1 - b0, tmp, nullptr, nullptr);
+      if (threadIdx.x == 0) rowc[r] = int32_t(n);
+    }
+    __syncthreads();
+  }
+}
+
 template <typename PTA, typename PTB, typename VT>
 static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                       const tspg_csr *B, tspg_csr_out *C) {
   const int64_t m = A->nrows;
   Scratch sc(ctx, s);
   int32_t *rowc, *dpre;
-  int64_t *cp, *partial;
+  int64_t *cp, *partial, *heavy;
   const int64_t nb = (m + kScanTile - 1) / kScanTile;
   Sched *dummy;
   TSPG_TRY(sc.get(&rowc, m));
@@ -123,16 +216,24 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   TSPG_TRY(sc.get(&cp, m + 1));
   TSPG_TRY(sc.get(&partial, nb + 1));
   TSPG_TRY(sc.get(&dummy, 1));
+  // heavy[0] = count of listed rows, heavy[1..] = the rows
+  const int64_t max_heavy = (A->nnz + B->nnz) / (kMergeHeavy + 1) + 1;
+  TSPG_TRY(sc.get(&heavy, max_heavy + 1));
+  TSPG_CUDA(ctx, cudaMemsetAsync(heavy, 0, sizeof(int64_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(cp, 0, sizeof(int64_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(dummy, 0, sizeof(Sched), s));
   const unsigned grid = (unsigned)std::min<int64_t>((m * 32 + 255) / 256, int64_t(ctx->num_sms) * 16);
   if (m > 0) {
     k_spadd_count<PTA, PTB><<<grid, 256, 0, s>>>(m, (const PTA *)A->rowptr, A->col,
-                                                 (const PTB *)B->rowptr, B->col, rowc);
+                                                 (const PTB *)B->rowptr, B->col, rowc,
+                                                 heavy + 1, heavy);
+    k_spadd_heavy<false, PTA, PTB, VT><<<ctx->num_sms * 2, kMergeThreads, 0, s>>>(
+        heavy + 1, heavy, (const PTA *)A->rowptr, A->col, (const VT *)A->val,
+        (const PTB *)B->rowptr, B->col, (const VT *)B->val, rowc, nullptr, nullptr, nullptr);
     k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial);
     k_scan_partials<<<1, 1024, 0, s>>>(partial, nb);
     k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial, nb, cp, dummy, nullptr);
-    ctx->launches += 4;
+    ctx->launches += 5;
   }
   TSPG_CUDA(ctx, cudaGetLastError());
   int64_t *h = ctx->h_words;
@@ -157,7 +258,10 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   k_spadd_fill<PTA, PTB, VT><<<grid, 256, 0, s>>>(
       m, (const PTA *)A->rowptr, A->col, (const VT *)A->val, (const PTB *)B->rowptr,
       B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val, dpre);
-  ctx->launches += 1;
+  k_spadd_heavy<true, PTA, PTB, VT><<<ctx->num_sms * 2, kMergeThreads, 0, s>>>(
+      heavy + 1, heavy, (const PTA *)A->rowptr, A->col, (const VT *)A->val,
+      (const PTB *)B->rowptr, B->col, (const VT *)B->val, nullptr, cp, C->col, (VT *)C->val);
+  ctx->launches += 2;
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
 }
