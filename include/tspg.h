@@ -30,8 +30,8 @@
  *   - Output rows of SpGEMM, SpGEMM-accumulate and spadd are sorted by column
  *     with no duplicate columns.  Structural zeros are kept (an entry whose
  *     value cancels to 0.0 stays in the pattern), matching KokkosKernels and
- *     csrgeam2 as Trident uses them.  spadd and the C_in operand of
- *     tspg_spgemm_acc require sorted, duplicate-free rows.
+ *     csrgeam2 as Trident uses them.  spadd requires sorted, duplicate-free
+ *     rows; the C_in operand of tspg_spgemm_acc may have either.
  */
 #ifndef TSPG_H
 #define TSPG_H
@@ -68,7 +68,13 @@ enum {
   /* Skip the device check that B's rows are sorted; the caller promises they
      are.  Without it the library checks and, for unsorted B, uses the
      cursor-free form of the long-row kernel. */
-  TSPG_F_B_SORTED = 1
+  TSPG_F_B_SORTED = 1,
+  /* tspg_spgemm_acc: force one SpGEMM with C_in's entries as products
+     (ACC_FUSE) or a product followed by the merge (ACC_SPLIT).  Default: fuse
+     when nnz(C_in) <= nnz(A) + nnz(B) — a large accumulator merges faster
+     (sequential) than it re-enters the hash / bitmap passes. */
+  TSPG_F_ACC_FUSE = 2,
+  TSPG_F_ACC_SPLIT = 4
 };
 
 /* Read-only sparse operand (CSR; for the pack, the compressed dimension is
@@ -200,7 +206,11 @@ int tspg_plan_destroy(tspg_plan *plan);
  * LocalMatrix::sp_mma (include/KokkosWrap.hpp:315-364), sp_mma_hybrid
  * (include/cusparse_helpers.cuh:708-739) and cusparse_spmma
  * (include/cusparse_helpers.cuh:744-796).  C_in may be NULL or empty (the
- * "first product" case, KokkosWrap.hpp:334-338); then C_out = A·B. */
+ * "first product" case, KokkosWrap.hpp:334-338); then C_out = A·B.  Either
+ * one SpGEMM in which C_in's entries join their rows as products with
+ * coefficient 1, or the product followed by tspg_spadd (flags
+ * TSPG_F_ACC_FUSE / TSPG_F_ACC_SPLIT; by default by size).  C_out's arrays
+ * must not overlap C_in's. */
 int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
                     const tspg_csr *B, const tspg_csr *C_in,
                     tspg_csr_out *C_out, int flags);

@@ -9,7 +9,7 @@ import torch
 import oracle
 from helpers import check_product, check_sum, random_csr
 from trident_b200 import ops, workloads
-from trident_b200._lib import TSPG_COLS, TSPG_ROWS
+from trident_b200._lib import TSPG_COLS, TSPG_F_ACC_FUSE, TSPG_F_ACC_SPLIT, TSPG_ROWS
 from trident_b200.csr import HostCSR
 
 pytestmark = pytest.mark.gpu
@@ -84,6 +84,58 @@ def test_sp_mma_accumulates_stages(ctx):
     np.testing.assert_array_equal(H.rowptr, ref.rowptr)
     np.testing.assert_array_equal(H.col, ref.col)
     np.testing.assert_allclose(H.val, ref.val, rtol=1e-12, atol=1e-12)
+
+
+def _acc_reference(A, B, E):
+    """E + A·B: E canonicalised (rows sorted, duplicates summed), then the
+    oracle's union merge with the oracle's product."""
+    import scipy.sparse as sp
+    rp, cj, cx, _ = oracle.spgemm(A, B)
+    P = HostCSR(A.nrows, B.ncols, rp, cj, cx)
+    S = sp.csr_matrix((E.val, E.col, E.rowptr), shape=(E.nrows, E.ncols))
+    S.sum_duplicates()
+    S.sort_indices()
+    Ec = HostCSR(E.nrows, E.ncols, S.indptr.astype(np.int64), S.indices.astype(np.int32), S.data)
+    cp, cj2, cx2 = oracle.spadd(P, Ec)
+    return HostCSR(A.nrows, B.ncols, cp, cj2, cx2)
+
+
+def _check_acc(C, ref):
+    H = C.to_host()
+    np.testing.assert_array_equal(H.rowptr.astype(np.int64), ref.rowptr)
+    np.testing.assert_array_equal(H.col, ref.col)
+    np.testing.assert_allclose(H.val, ref.val, rtol=1e-12, atol=1e-11)
+
+
+@pytest.mark.parametrize("mode", [TSPG_F_ACC_FUSE, TSPG_F_ACC_SPLIT])
+def test_sp_mma_fused_all_row_forms(ctx, mode):
+    # C_in joins every row form: R-MAT rows (warp ... DENSE), rows where A is
+    # empty but C_in is not, and C_in rows unsorted with repeated columns
+    # (the split form merges, so its C_in must be canonical)
+    R = workloads.rmat(scale=12, edge_factor=16, seed=8)
+    E = random_csr(R.nrows, R.ncols, density=0.003, seed=10)
+    _check_acc(ops.sp_mma(ctx, R.to_device(), R.to_device(), E.to_device(), flags=mode),
+               _acc_reference(R, R, E))
+    if mode != TSPG_F_ACC_FUSE:
+        return
+    A0 = random_csr(500, 400, density=0.01, seed=11)
+    cut = A0.rowptr[100]  # rows 0..99 of A emptied
+    rp = np.concatenate([np.zeros(100, np.int64), A0.rowptr[100:] - cut])
+    A = HostCSR(A0.nrows, A0.ncols, rp, A0.col[cut:], A0.val[cut:])
+    B = random_csr(400, 700, density=0.02, seed=12)
+    Ed = random_csr(500, 700, per_row=30, seed=13, sort=False, dup=True)
+    _check_acc(ops.sp_mma(ctx, A.to_device(), B.to_device(), Ed.to_device(), flags=mode),
+               _acc_reference(A, B, Ed))
+
+
+def test_sp_mma_fused_wide_b(ctx):
+    # the windowed DENSE form (ncols above the whole-row bitmap) with an addend
+    n = 1_250_000
+    B = random_csr(2000, n, per_row=30, seed=14)
+    A = random_csr(5, 2000, per_row=900, seed=15)
+    E = random_csr(5, n, per_row=5000, seed=16)
+    _check_acc(ops.sp_mma(ctx, A.to_device(), B.to_device(), E.to_device(), flags=TSPG_F_ACC_FUSE),
+               _acc_reference(A, B, E))
 
 
 def test_gen_bitmask_kats(ctx):

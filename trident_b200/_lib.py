@@ -16,6 +16,7 @@ TSPG_OK, TSPG_EINVAL, TSPG_ENOMEM, TSPG_EOVERFLOW, TSPG_ETIMEOUT, TSPG_ECUDA, TS
 TSPG_PACK_NOALLOC_MAX_SEGMENTS = 262144
 TSPG_ROWS, TSPG_COLS = 0, 1
 TSPG_F_B_SORTED = 1
+TSPG_F_ACC_FUSE, TSPG_F_ACC_SPLIT = 2, 4
 
 
 class TspgCsr(C.Structure):

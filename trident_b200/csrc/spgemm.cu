@@ -56,6 +56,7 @@ struct tspg_plan {
   int32_t *curbuf = nullptr;
   int64_t cur_stride = 0;
   int64_t *wide_a = nullptr, *wide_b = nullptr;  // widened row offsets (mixed widths)
+  tspg_csr E{};        // addend of C = E + A·B (tspg_spgemm_acc), E.col == nullptr if none
   void *blocks[16];
   int nblocks = 0;
 
@@ -121,6 +122,12 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   v.n = n;
   v.cp_bits = 64;
   v.b_sorted = 1;
+  if (P->E.col && P->E.nnz > 0) {
+    v.Ep = P->E.rowptr;
+    v.Ej = P->E.col;
+    v.Ex = (const VT *)P->E.val;
+    v.ep_bits = P->E.rowptr_bits;
+  }
   k_set_prod<PT, VT><<<1, 1, 0, s>>>(prods, v, P->base, m);
   if (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) {
     k_check_sorted_rows<PT><<<grid_for(B->nrows * 32, 256, ctx->num_sms * 16), 256,
@@ -245,10 +252,11 @@ static int plan_get(tspg_ctx *, void *plan, int64_t **p, int64_t n) {
   return ((tspg_plan *)plan)->get(p, size_t(n));
 }
 
-extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
-                                    const tspg_csr *A_in, const tspg_csr *B_in,
-                                    int flags, tspg_plan **plan,
-                                    int64_t *c_nnz) {
+// Symbolic phase of A·B, or of E + A·B when E is given (its entries join
+// their rows as products with coefficient 1).
+static int symbolic_entry(tspg_ctx *ctx, void *stream, const tspg_csr *A_in,
+                          const tspg_csr *B_in, const tspg_csr *E, int flags,
+                          tspg_plan **plan, int64_t *c_nnz) {
   if (!ctx || !plan) return TSPG_EINVAL;
   *plan = nullptr;
   TSPG_TRY(check_pair(A_in, B_in));
@@ -258,6 +266,7 @@ extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
   if (!P) return TSPG_ENOMEM;
   P->ctx = ctx;
   P->stream = s;
+  if (E) P->E = *E;
   tspg_csr a = *A_in, b = *B_in;
   const tspg_csr *A = &a, *B = &b;
   if (a.rowptr_bits != b.rowptr_bits) {
@@ -288,6 +297,13 @@ extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
   if (c_nnz) *c_nnz = P->c_nnz;
   *plan = P;
   return TSPG_OK;
+}
+
+extern "C" int tspg_spgemm_symbolic(tspg_ctx *ctx, void *stream,
+                                    const tspg_csr *A_in, const tspg_csr *B_in,
+                                    int flags, tspg_plan **plan,
+                                    int64_t *c_nnz) {
+  return symbolic_entry(ctx, stream, A_in, B_in, nullptr, flags, plan, c_nnz);
 }
 
 extern "C" int tspg_spgemm_numeric(tspg_ctx *ctx, void *stream,
@@ -425,15 +441,29 @@ extern "C" int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
   if (!ctx) return TSPG_EINVAL;
   TSPG_TRY(check_pair(A, B));
   const bool have_in = C_in && C_in->nnz > 0;
-  if (!have_in) return tspg_spgemm(ctx, stream, A, B, C_out, flags);
+  const int pflags = flags & TSPG_F_B_SORTED;
+  if (!have_in) return tspg_spgemm(ctx, stream, A, B, C_out, pflags);
   TSPG_TRY(check_csr(C_in));
   if (C_in->nrows != A->nrows || C_in->ncols != B->ncols ||
       C_in->val_bits != A->val_bits)
     return TSPG_EINVAL;
+  TSPG_TRY(check_out(C_out, A->nrows, B->ncols, A->val_bits));
+  const bool fuse = (flags & TSPG_F_ACC_FUSE) ||
+                    (!(flags & TSPG_F_ACC_SPLIT) && C_in->nnz <= A->nnz + B->nnz);
+  if (fuse) {
+    // one SpGEMM in which C_in's entries join their rows as products with
+    // coefficient 1
+    tspg_plan *plan = nullptr;
+    TSPG_TRY(symbolic_entry(ctx, stream, A, B, C_in, pflags, &plan, nullptr));
+    const int st = tspg_spgemm_numeric(ctx, stream, plan, A, B, C_out);
+    tspg_plan_destroy(plan);
+    return st;
+  }
+  // the product into workspace, then the merge into C_out
   cudaStream_t s = (cudaStream_t)stream;
   tspg_plan *plan = nullptr;
   int64_t nnz = 0;
-  TSPG_TRY(tspg_spgemm_symbolic(ctx, stream, A, B, flags, &plan, &nnz));
+  TSPG_TRY(tspg_spgemm_symbolic(ctx, stream, A, B, pflags, &plan, &nnz));
   const int vb = A->val_bits / 8;
   const int pb = nnz > INT32_MAX ? 64 : C_in->rowptr_bits;
   void *rp = nullptr, *cj = nullptr, *cx = nullptr;
@@ -456,9 +486,6 @@ extern "C" int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
   if (st == TSPG_OK) {
     tspg_csr prod{T.nrows, T.ncols, T.nnz, T.rowptr, T.rowptr_bits, T.val_bits,
                   T.col, T.val};
-    if (prod.nnz == 0) {
-      // nothing to add: C_out = C_in (through the merge with an empty operand)
-    }
     st = tspg_spadd(ctx, stream, &prod, C_in, C_out);
   }
   ws_free(ctx, cx, s);

@@ -100,7 +100,25 @@ struct ProdDev {
   void *Cp;       // output rowptr (product-local), cp_bits wide
   int32_t cp_bits;
   int32_t b_sorted;
+  // optional addend of C = E + A·B (tspg_spgemm_acc): E's row r joins row r's
+  // products as entries with coefficient 1; Ej == nullptr when there is none
+  const void *Ep;
+  const int32_t *Ej;
+  const VT *Ex;
+  int32_t ep_bits;
 };
+
+template <typename PT, typename VT>
+__device__ __forceinline__ void addend_row(const ProdDev<PT, VT> &P, int64_t r, int64_t &e0,
+                                           int64_t &e1) {
+  if (P.ep_bits == 32) {
+    e0 = ((const int32_t *)P.Ep)[r];
+    e1 = ((const int32_t *)P.Ep)[r + 1];
+  } else {
+    e0 = ((const int64_t *)P.Ep)[r];
+    e1 = ((const int64_t *)P.Ep)[r + 1];
+  }
+}
 
 // Work schedule of one phase: rows per class, their list offsets and the
 // work-item prefix the persistent kernel decodes.
@@ -187,8 +205,16 @@ static __global__ void k_widen(const int32_t *src, int64_t n, int64_t *dst) {
 template <typename PT, typename VT>
 __global__ void k_set_operands(ProdDev<PT, VT> *dst, ProdDev<PT, VT> v) {
   const int32_t sorted = dst->b_sorted;
+  const void *ep = dst->Ep;  // the addend stays the symbolic call's
+  const int32_t *ej = dst->Ej;
+  const VT *ex = dst->Ex;
+  const int32_t eb = dst->ep_bits;
   *dst = v;
   dst->b_sorted = sorted;
+  dst->Ep = ep;
+  dst->Ej = ej;
+  dst->Ex = ex;
+  dst->ep_bits = eb;
 }
 
 template <typename PT, typename VT>
@@ -249,6 +275,11 @@ __global__ void __launch_bounds__(256) k_row_mults(
     }
     f = warp_sum(f);
     if (lane == 0) {
+      if (prods[p].Ej) {  // the addend's entries count as products of the row
+        int64_t e0, e1;
+        addend_row(prods[p], r, e0, e1);
+        f += e1 - e0;
+      }
       rowf[g] = f;
       const int64_t n = prods[p].n;
       const int c = sym_class(f, n, S->tune);

@@ -186,6 +186,20 @@ __device__ __forceinline__ void for_products_flat(
   }
 }
 
+// The addend row of C = E + A·B (ProdDev::Ej; nothing when there is none):
+// fn(col, value) for E's row r, lanes lane, lane + G, ...
+template <bool NUM, typename PT, typename VT, typename F>
+__device__ __forceinline__ void for_addend(const ProdDev<PT, VT> &P, int64_t r, int lane,
+                                           int G, F &&fn) {
+  if (!P.Ej) return;
+  int64_t e0, e1;
+  addend_row(P, r, e0, e1);
+  for (int64_t q = e0 + lane; q < e1; q += G) {
+    if constexpr (NUM) fn(__ldg(P.Ej + q), __ldg(P.Ex + q));
+    else fn(__ldg(P.Ej + q), VT(0));
+  }
+}
+
 // Probe bound: tables are sized T >= 2 * (distinct keys), so a probe never
 // runs T steps; the bound only turns a broken invariant into an error flag.
 __device__ __forceinline__ int sym_insert(int *keys, int32_t col, int logT,
@@ -318,6 +332,7 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     for_products_balanced<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane,
                                             gid, gm.lst, gm.nl, gm.cap, ins);
   }
+  for_addend<false>(P, rr.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
   const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
@@ -344,16 +359,17 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     const int64_t nw = (w1 - w0 + 31) >> 5;
     for (int64_t i = tid; i < nw; i += kThreads) bm[i] = 0u;
     __syncthreads();
-    for_products_balanced<kThreads, false, PT, VT>(
-        P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl, gm.cap,
-        [&](int32_t col, VT) {
-          if (col >= w0 && col < w1) {
-            const uint32_t o = uint32_t(col - w0);
-            const uint32_t bit = 1u << (o & 31);
-            if (!(((volatile uint32_t *)bm)[o >> 5] & bit))
-              atomicOr(bm + (o >> 5), bit);
-          }
-        });
+    auto mark = [&](int32_t col, VT) {
+      if (col >= w0 && col < w1) {
+        const uint32_t o = uint32_t(col - w0);
+        const uint32_t bit = 1u << (o & 31);
+        if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
+      }
+    };
+    for_products_balanced<kThreads, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
+                                                   A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl,
+                                                   gm.cap, mark);
+    for_addend<false>(P, rr.r, tid, kThreads, mark);
     __syncthreads();
     int64_t local = 0;
     for (int64_t i = tid; i < nw; i += kThreads) local += __popc(bm[i]);
@@ -496,6 +512,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                                            A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl, gm.cap,
                                            ins);
   }
+  for_addend<true>(P, rr.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
@@ -620,13 +637,14 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   long long tp = clock64();
   for (int i = tid; i < nb * 32; i += kThreads) bm[i] = 0u;
   __syncthreads();
-  for_products_balanced<kThreads, false, PT, VT>(
-      Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
-      [&](int32_t col, VT) {
-        const uint32_t bit = 1u << (col & 31);
-        uint32_t &x = bmw(col >> 5);
-        if (!(*(volatile uint32_t *)&x & bit)) atomicOr(&x, bit);
-      });
+  auto mark = [&](int32_t col, VT) {
+    const uint32_t bit = 1u << (col & 31);
+    uint32_t &x = bmw(col >> 5);
+    if (!(*(volatile uint32_t *)&x & bit)) atomicOr(&x, bit);
+  };
+  for_products_balanced<kThreads, false, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
+                                                 gm.lst, gm.nl, gm.cap, mark);
+  for_addend<false>(P, rr.r, tid, kThreads, mark);
   __syncthreads();
   prof_sub(A, 0, tp);
   // Block scan: block b = words [32b, 32b + 32), lane l of a warp takes word
@@ -714,9 +732,10 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     const int w = col >> 5;
     return bbase[w >> 5] + int(wp[w]) + __popc(bmw(w) & ((1u << (col & 31)) - 1u));
   };
-  for_products_balanced<kThreads, true, PT, VT>(
-      Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0, gm.lst, gm.nl, gm.cap,
-      [&](int32_t col, VT v) { red_add(Cx + rank_of(col), v); });
+  auto put = [&](int32_t col, VT v) { red_add(Cx + rank_of(col), v); };
+  for_products_balanced<kThreads, true, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
+                                                gm.lst, gm.nl, gm.cap, put);
+  for_addend<true>(P, rr.r, tid, kThreads, put);
   __syncthreads();
   prof_sub(A, 4, tp);
 }
@@ -831,6 +850,10 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
         }
       }
     }
+    // the addend row: every window scans it and takes its own columns
+    for_addend<true>(P, rr.r, tid, kThreads, [&](int32_t col, VT v) {
+      if (col >= w0 && col < w1) add(int32_t(col - w0), v);
+    });
     if (A.prof) __syncthreads();  // profiling only: split short / long walks
     prof_sub(A, 6, tp);
     // long entries: warp w walks listed entries w, w + 16, ...; its lanes take
