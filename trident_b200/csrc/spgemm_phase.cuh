@@ -13,6 +13,8 @@
 //      barriers.
 #pragma once
 
+#include <type_traits>
+
 #include "spgemm_kernels.cuh"
 
 namespace tspg {
@@ -125,18 +127,28 @@ __device__ __forceinline__ void for_products_flat(
   int64_t *spre = (int64_t *)stage;
   int64_t *sb0 = spre + G;
   VT *sa = (VT *)(sb0 + G);
+  // positions fit 32 bits when B's row offsets do (nnz(B) < 2^31): the warp
+  // form then shuffles half the words
+  using IX = std::conditional_t<G == 32 && sizeof(PT) == 4, int32_t, int64_t>;
   for (int64_t c0 = a0; c0 < a1; c0 += G) {
     const int nc = int(min(int64_t(G), a1 - c0));
-    int64_t len = 0, b0 = 0;
+    IX len = 0, b0 = 0;
     VT a = VT(0);
     if (lane < nc) {
       const int64_t k = __ldg(Aj + c0 + lane);
       if constexpr (NUM) a = __ldg(Ax + c0 + lane);
-      b0 = __ldg(Bp + k);
-      len = __ldg(Bp + k + 1) - b0;
+      b0 = IX(__ldg(Bp + k));
+      len = IX(__ldg(Bp + k + 1)) - b0;
     }
-    int64_t tot;
-    const int64_t pre = group_excl_scan<G, int64_t>(len, tmp, gid, &tot);
+    IX tot;
+    IX pre;
+    if constexpr (G == 32) {
+      const IX inc = warp_scan_incl(len);
+      tot = __shfl_sync(0xffffffffu, inc, 31);
+      pre = inc - len;
+    } else {
+      pre = group_excl_scan<G, int64_t>(len, tmp, gid, &tot);
+    }
     if constexpr (G != 32) {
       if (lane < nc) {
         spre[lane] = pre;
@@ -146,18 +158,18 @@ __device__ __forceinline__ void for_products_flat(
       group_sync<G>(gid);
     }
     // the step loop is uniform across the group (the G = 32 search shuffles)
-    for (int64_t pb = 0; pb < tot; pb += int64_t(G) * U) {
+    for (IX pb = 0; pb < tot; pb += IX(G) * U) {
       int32_t cc[U];
       VT xv[U], av[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int64_t p = pb + int64_t(u) * G + lane;
+        const IX p = pb + IX(u) * G + lane;
         int j = 0;
-        int64_t pj, bj;
+        IX pj, bj;
         if constexpr (G == 32) {
 #pragma unroll
           for (int st = 16; st > 0; st >>= 1) {
-            const int64_t v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
+            const IX v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
             if (j + st < nc && v <= p) j += st;
           }
           pj = __shfl_sync(0xffffffffu, pre, j);
@@ -170,7 +182,7 @@ __device__ __forceinline__ void for_products_flat(
           bj = sb0[j];
           if constexpr (NUM) av[u] = sa[j];
         }
-        const int64_t q = bj + (p - pj);
+        const IX q = bj + (p - pj);
         cc[u] = p < tot ? __ldg(Bj + q) : -1;
         if constexpr (NUM) xv[u] = p < tot ? __ldg(Bx + q) : VT(0);
       }
