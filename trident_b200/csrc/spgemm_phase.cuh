@@ -615,6 +615,168 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   prof_sub_g(A, 13, tp, lane == 0);
 }
 
+// Numeric group row by expand-sort-compress, for rows with at most TMAX / 2
+// products of which few repeat a column (the uniform-random rows of batched
+// products): the products (and the addend row) are written to the slice in
+// product order, sorted by column (the row radix sort), and runs of equal
+// columns are summed as they are written out.  No hash table to clear, probe
+// or compact; the sort sees f <= 1.5 c entries instead of c.
+template <int G, int TMAX, typename PT, typename VT>
+__device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, int64_t idx,
+                            unsigned char *slice, const GroupMem &gm, int gid, int lane) {
+  constexpr int U = 4, FMAX = TMAX / 2, KEEP = TMAX / (2 * G);
+  VT *vals = (VT *)slice;  // [0, FMAX) and [FMAX, TMAX): the sort's two buffers
+  int *keys = (int *)(slice + TMAX * 8);
+  int64_t *spre = (int64_t *)gm.stage;  // G > 32: the chunk's entries
+  int64_t *sb0 = spre + G;
+  VT *sa = (VT *)(sb0 + G);
+  long long tp = clock64();
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
+  const int64_t c = A.rowc[rr.g];
+  const int f = int(A.rowf[rr.g]);  // <= FMAX by the caller's test
+  const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  prof_sub_g(A, 9, tp, lane == 0);
+  // expand: every product at its flat index
+  int fb = 0;
+  for (int64_t c0 = a0; c0 < a1; c0 += G) {
+    const int nc = int(min(int64_t(G), a1 - c0));
+    int64_t len = 0, b0 = 0;
+    VT a = VT(0);
+    if (lane < nc) {
+      const int64_t k = __ldg(P.Aj + c0 + lane);
+      a = __ldg(P.Ax + c0 + lane);
+      b0 = int64_t(__ldg(P.Bp + k));
+      len = int64_t(__ldg(P.Bp + k + 1)) - b0;
+    }
+    int64_t tot, pre;
+    if constexpr (G == 32) {
+      const int64_t inc = warp_scan_incl(len);
+      tot = __shfl_sync(0xffffffffu, inc, 31);
+      pre = inc - len;
+    } else {
+      pre = group_excl_scan<G, int64_t>(len, gm.tmp, gid, &tot);
+      if (lane < nc) {
+        spre[lane] = pre;
+        sb0[lane] = b0;
+        sa[lane] = a;
+      }
+      group_sync<G>(gid);
+    }
+    for (int64_t pb = 0; pb < tot; pb += int64_t(G) * U) {
+      int32_t cc[U];
+      VT xv[U], av[U];
+      int64_t at[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t p = pb + int64_t(u) * G + lane;
+        int j = 0;
+        int64_t pj, bj;
+        if constexpr (G == 32) {
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const int64_t v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
+            if (j + st < nc && v <= p) j += st;
+          }
+          pj = __shfl_sync(0xffffffffu, pre, j);
+          bj = __shfl_sync(0xffffffffu, b0, j);
+          av[u] = __shfl_sync(0xffffffffu, a, j);
+        } else {
+          for (int st = G / 2; st > 0; st >>= 1)
+            if (j + st < nc && spre[j + st] <= p) j += st;
+          pj = spre[j];
+          bj = sb0[j];
+          av[u] = sa[j];
+        }
+        const int64_t q = bj + (p - pj);
+        at[u] = p < tot ? fb + p : -1;
+        cc[u] = p < tot ? __ldg(P.Bj + q) : 0;
+        xv[u] = p < tot ? __ldg(P.Bx + q) : VT(0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (at[u] >= 0 && at[u] < FMAX) {
+          keys[at[u]] = cc[u];
+          vals[at[u]] = av[u] * xv[u];
+        }
+      }
+    }
+    fb += int(tot);
+    group_sync<G>(gid);  // the next chunk reuses the staging
+  }
+  if (P.Ej) {
+    int64_t e0, e1;
+    addend_row(P, rr.r, e0, e1);
+    for (int64_t q = e0 + lane; q < e1; q += G) {
+      const int64_t at = fb + (q - e0);
+      if (at < FMAX) {
+        keys[at] = __ldg(P.Ej + q);
+        vals[at] = __ldg(P.Ex + q);
+      }
+    }
+    fb += int(e1 - e0);
+  }
+  group_sync<G>(gid);
+  if (lane == 0 && fb != f) set_error(A.err, 107);
+  prof_sub_g(A, 10, tp, lane == 0);
+  int mn = INT32_MAX, mx = -1;
+  for (int e = lane; e < f; e += G) {
+    mn = min(mn, keys[e]);
+    mx = max(mx, keys[e]);
+  }
+  group_minmax<G>(mn, mx, gm.itmp, gid);
+  int src = 0, bias = 0;
+  if (f <= kBitonicMax) {
+    const uint32_t Pw = pow2_at_least(f, 2);
+    for (uint32_t e = uint32_t(f) + lane; e < Pw; e += G) keys[e] = INT32_MAX;
+    group_sync<G>(gid);
+    prof_sub_g(A, 11, tp, lane == 0);
+    bitonic_pairs<G, VT>(keys, vals, Pw, gid, lane);
+  } else {
+    bias = mn;
+    for (int e = lane; e < f; e += G) keys[e] -= bias;
+    group_sync<G>(gid);
+    prof_sub_g(A, 11, tp, lane == 0);
+    const int bits = mx > mn ? 32 - __clz(mx - mn) : 1;
+    if (KEEP >= 4 && f <= 4 * G)
+      src = radix_pairs<G, (KEEP < 4 ? KEEP : 4), (KEEP < 4 ? 5 : 7), VT>(
+          keys, vals, keys + FMAX, vals + FMAX, f, bits, gm.cnt, gm.tmp, gid, lane);
+    else if (KEEP >= 8 && f <= 8 * G)
+      src = radix_pairs<G, (KEEP < 8 ? KEEP : 8), (KEEP < 8 ? 5 : 6), VT>(
+          keys, vals, keys + FMAX, vals + FMAX, f, bits, gm.cnt, gm.tmp, gid, lane);
+    else
+      src = radix_pairs<G, 16, 5, VT>(keys, vals, keys + FMAX, vals + FMAX, f, bits, gm.cnt,
+                                      gm.tmp, gid, lane);
+  }
+  prof_sub_g(A, 12, tp, lane == 0);
+  // compress: the first entry of every run of equal columns sums its run
+  const int *ko = src ? keys + FMAX : keys;
+  const VT *vo = src ? vals + FMAX : vals;
+  int32_t *__restrict__ Cj = P.Cj + off;
+  VT *__restrict__ Cx = P.Cx + off;
+  int64_t running = 0;
+  for (int e0 = 0; e0 < f; e0 += G) {
+    const int e = e0 + lane;
+    const int key = e < f ? ko[e] : 0;
+    const bool head = e < f && (e == 0 || ko[e - 1] != key);
+    int64_t ctot;
+    const int64_t pos = running + group_excl_scan<G, int64_t>(head ? 1 : 0, gm.tmp, gid, &ctot);
+    if (head) {
+      VT v = vo[e];
+      for (int k = e + 1; k < f && ko[k] == key; ++k) v += vo[k];
+      if (pos < c) {
+        Cj[pos] = key + bias;
+        Cx[pos] = v;
+      }
+    }
+    running += ctot;
+  }
+  if (lane == 0 && running != c) set_error(A.err, 108);
+  group_sync<G>(gid);
+  prof_sub_g(A, 13, tp, lane == 0);
+}
+
 // DENSE numeric row, whole-row form (ncols <= kRankMaxCols).  Pass 1 sets the
 // row's column bitmap; a CTA scan of the bitmap gives every word's rank base
 // (block base + uint16 offset inside the block); the row's values are zeroed
@@ -937,6 +1099,16 @@ struct PhaseShared {
   int64_t off[NCLS], cnt[NCLS];
 };
 
+// Group rows that take the expand-sort-compress form: at most fmax products
+// (half the group's table), and at most 1.5 products per output (few
+// repeated columns).
+__device__ __forceinline__ bool esc_fits(const PhaseArgs &A, int64_t idx, int64_t fmax) {
+  const uint64_t e = A.list[idx];
+  const int64_t g = A.base[int(e >> 40)] + int64_t(e & ((uint64_t(1) << 40) - 1));
+  const int64_t f = A.rowf[g], c = A.rowc[g];
+  return f <= fmax && 2 * f <= 3 * c;
+}
+
 // Group-level rows of class `cls`: the group leader fetches one row index at a
 // time; the group exits when the class runs out.
 template <int G, bool NUM, typename PT, typename VT>
@@ -987,10 +1159,14 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       const int64_t e = min(count, i + take);
       for (; i < e; ++i) {
         const long long t0 = clock64();
-        if constexpr (NUM)
-          num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
-        else
+        if constexpr (NUM) {
+          if (esc_fits(A, base + i, TMAXN / 2))
+            num_esc_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+          else
+            num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+        } else {
           sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+        }
         prof_add(A, cls, t0, lane == 0);
       }
     } else {
@@ -1008,9 +1184,12 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       const int64_t e = min(count, i + int64_t(v >> 48));
       for (; i < e; ++i) {
         const long long t0 = clock64();
-        if constexpr (NUM)
-          num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
-        else
+        if constexpr (NUM) {
+          if (esc_fits(A, base + i, TMAXN / 2))
+            num_esc_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+          else
+            num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+        } else
           sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
         prof_add(A, cls, t0, lane == 0);
       }
