@@ -201,3 +201,16 @@ def test_mixed_rowptr_widths(ctx):
     p = ops.Plan(ctx, A.to_device(rowptr_bits=32), B.to_device(rowptr_bits=64))
     check_product(p.numeric(A.to_device(rowptr_bits=32), B.to_device(rowptr_bits=64)), A, B)
     p.close()
+
+
+@pytest.mark.parametrize("lam", [6.0, 20.0, 40.0])
+def test_uniform_rows_expand_sort_compress(ctx, lam):
+    # Poisson rows of uniform-random columns have almost no repeated columns,
+    # so warp, 128- and 256-thread rows take the expand-sort-compress form
+    # (lam 40: ~1600 outputs per row, 256-thread rows)
+    A, B = workloads.batched_product((3000, lam, 71, 72))
+    check_product(ops.spgemm(ctx, A.to_device(), B.to_device()), A, B)
+    r32 = lambda M: HostCSR(M.nrows, M.ncols, M.rowptr, M.col,
+                            M.val.astype(np.float32).astype(np.float64))
+    C32 = ops.spgemm(ctx, A.to_device(val_bits=32), B.to_device(val_bits=32))
+    check_product(C32, r32(A), r32(B), tol=TOL32)
