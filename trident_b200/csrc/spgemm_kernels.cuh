@@ -63,6 +63,11 @@ constexpr int kBitonicMax = 64;          // rows up to this size sort bitonic
 // whole-row DENSE numeric form: per 32 columns a bitmap word (4 B) and a
 // uint16 rank offset, per 1024 columns an int block base (196 B per block)
 constexpr int64_t kRankMaxCols = int64_t(kDynSmem / 196) * 1024;
+// numeric CTA-level rows: at most one heavy (DENSE0 / DENSE1) row per this
+// many items; the period is also capped at 1 + light / heavy rows, so in
+// practice the heavy rows spread evenly over the whole item sequence (R-MAT
+// 20: 309.9 ms heaviest-first, 299.7 / 292.5 / 289.7 ms with periods 4 / 8 / 11)
+constexpr int kHeavyPeriod = 64;
 
 __host__ __device__ inline int dense_sub(int64_t f) {
   return f >= (int64_t(1) << 20) ? CLS_DENSE0 : f >= (int64_t(1) << 17) ? CLS_DENSE1 : CLS_DENSE2;

@@ -1232,9 +1232,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int64_t item = (int64_t)sh.slot[15];
     __syncthreads();
     if (item >= s_items[kCtaClasses]) break;
+    // numeric: the heavy DENSE0 / DENSE1 rows (heaviest first) are interleaved
+    // with the lighter CTA rows, one in every K items, so fewer heavy rows are
+    // in flight at once and their output segments (the targets of the global
+    // reductions) stay in L2; symbolic: heaviest first
+    int64_t pos = item;
+    if (NUM) {
+      const int64_t H = s_items[2], L = s_items[kCtaClasses] - H;
+      int64_t K = H > 0 ? min(int64_t(kHeavyPeriod), 1 + L / H) : 1;
+      // (past the interleaved stretch the light rows follow in order: pos = item)
+      if (K > 1 && item < K * H) pos = item % K == 0 ? item / K : H + (item - item / K - 1);
+    }
     int c = 0;
-    while (item >= s_items[c + 1]) ++c;
-    const int64_t idx = sh.off[c] + (item - s_items[c]);
+    while (pos >= s_items[c + 1]) ++c;
+    const int64_t idx = sh.off[c] + (pos - s_items[c]);
     const long long t0 = clock64();
     if (cls_dense(c)) {
       if constexpr (NUM) {
