@@ -261,6 +261,37 @@ __device__ __forceinline__ void set_error(int64_t *err, int code) {
 __device__ __forceinline__ void red_add(double *p, double v) {
   asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
 }
+// L2 eviction-priority policies (PTX createpolicy) and the stores and
+// reductions that carry them.  evict_last marks lines that will be hit again
+// soon (a DENSE row's values, reduced into while the row is worked on),
+// evict_first lines written once (its column indices).
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void red_add_hint(double *p, double v, uint64_t pol) {
+  asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v),
+               "l"(pol) : "memory");
+}
+__device__ __forceinline__ void red_add_hint(float *p, float v, uint64_t pol) {
+  asm volatile("red.relaxed.gpu.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v),
+               "l"(pol) : "memory");
+}
+__device__ __forceinline__ void store_hint(double *p, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void store_hint(float *p, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void store_hint(int32_t *p, int32_t v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
+}
 __device__ __forceinline__ void red_add(float *p, float v) {
   asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }

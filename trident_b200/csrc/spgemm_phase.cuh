@@ -861,7 +861,9 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   int32_t *__restrict__ Cj = P.Cj + off;
   VT *__restrict__ Cx = P.Cx + off;
   // zeroed values: a contiguous range, coalesced
-  for (int64_t e = tid; e < c; e += kThreads) Cx[e] = VT(0);
+  // the values stay in L2 for the reductions, the indices may leave first
+  const uint64_t keep = policy_evict_last(), pass = policy_evict_first();
+  for (int64_t e = tid; e < c; e += kThreads) store_hint(Cx + e, VT(0), keep);
   prof_sub(A, 2, tp);
   // Column indices.  The bitmap walk is a merge of two sequences, the words
   // and the set bits (nw + c steps: every bit, then a step to the next word);
@@ -890,7 +892,8 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     uint32_t nxt = w + 1 < nw ? bmw(w + 1) : 0u;
     for (int64_t d = d0; d < d1; ++d) {
       if (word != 0u) {
-        if (e < c) Cj[e] = w * 32 + (__ffs(word) - 1);  // e < c unless rank sums broke
+        if (e < c)  // e < c unless rank sums broke
+          store_hint(Cj + e, int32_t(w * 32 + (__ffs(word) - 1)), pass);
         ++e;
         word &= word - 1u;
       } else {
@@ -906,7 +909,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     const int w = col >> 5;
     return bbase[w >> 5] + int(wp[w]) + __popc(bmw(w) & ((1u << (col & 31)) - 1u));
   };
-  auto put = [&](int32_t col, VT v) { red_add(Cx + rank_of(col), v); };
+  auto put = [&](int32_t col, VT v) { red_add_hint(Cx + rank_of(col), v, keep); };
   for_products_balanced<kThreads, true, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
                                                 gm.lst, gm.nl, gm.cap, put);
   for_addend<true>(P, rr.r, tid, kThreads, put);
