@@ -826,12 +826,26 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   // its block (< 1024), bbase[b] = rank of block b's first bit.
   {
     const int warp = tid >> 5, lane = tid & 31;
-    for (int b = warp; b < nb; b += kThreads / 32) {
-      const int w = (b << 5) + lane;
-      const int pc = w < nw ? __popc(bmw(w)) : 0;
-      const int inc = warp_scan_incl(pc);
-      if (w < nw) wp[w] = uint16_t(inc - pc);
-      if (lane == 31) bbase[b] = inc;
+    // four blocks per step: their scans are independent, so their shuffle
+    // latencies overlap
+    constexpr int NW = kThreads / 32, UB = 4;
+    for (int b0 = warp; b0 < nb; b0 += NW * UB) {
+      int pc[UB], inc[UB];
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int w = ((b0 + u * NW) << 5) + lane;
+        pc[u] = (b0 + u * NW < nb && w < nw) ? __popc(bmw(w)) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < UB; ++u) inc[u] = warp_scan_incl(pc[u]);
+#pragma unroll
+      for (int u = 0; u < UB; ++u) {
+        const int b = b0 + u * NW, w = (b << 5) + lane;
+        if (b < nb) {
+          if (w < nw) wp[w] = uint16_t(inc[u] - pc[u]);
+          if (lane == 31) bbase[b] = inc[u];
+        }
+      }
     }
   }
   __syncthreads();
@@ -889,7 +903,10 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     uint32_t word = bmw(w);
     // the lowest e - rank(w) set bits of this word belong to earlier threads
     for (int k = e - bbase[w >> 5] - int(wp[w]); k > 0; --k) word &= word - 1u;
-    uint32_t nxt = w + 1 < nw ? bmw(w + 1) : 0u;
+    // the next four words are loaded ahead, so runs of empty words do not
+    // wait on one shared-memory load per step
+    uint32_t n0 = w + 1 < nw ? bmw(w + 1) : 0u, n1 = w + 2 < nw ? bmw(w + 2) : 0u;
+    uint32_t n2 = w + 3 < nw ? bmw(w + 3) : 0u, n3 = w + 4 < nw ? bmw(w + 4) : 0u;
     for (int64_t d = d0; d < d1; ++d) {
       if (word != 0u) {
         if (e < c)  // e < c unless rank sums broke
@@ -898,8 +915,11 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
         word &= word - 1u;
       } else {
         ++w;
-        word = nxt;
-        nxt = w + 1 < nw ? bmw(w + 1) : 0u;
+        word = n0;
+        n0 = n1;
+        n1 = n2;
+        n2 = n3;
+        n3 = w + 4 < nw ? bmw(w + 4) : 0u;
       }
     }
   }
