@@ -163,20 +163,9 @@ __device__ __forceinline__ uint32_t pow2_at_least(int64_t x, uint32_t lo) {
   return t;
 }
 
-// Threads of a sub-group walk one B row together.  The width is chosen so
-// that every A entry of the row gets its own sub-group when the group is wide
-// enough (G / pow2 >= na): the dependent load chain A -> B rowptr -> B row is
-// then paid once per row instead of once per A entry; B rows longer than a
-// sub-group's share are walked by the whole group (for_products_balanced).
-__device__ __forceinline__ int subgroup_width(int64_t na, int G) {
-  int64_t p = 1;
-  while (p < na && p < G) p <<= 1;
-  int64_t S = G / p;
-  return int(S < 1 ? 1 : S > 32 ? 32 : S);
-}
-
-// Width from the average segment length (the cursor sweep of the windowed
-// DENSE form walks one window's segment per entry at a time).
+// Sub-group width for the CTA rows' product loop (for_products_balanced):
+// threads of a sub-group walk one B row together, sized to the row's average
+// B row length f / na.
 __device__ __forceinline__ int subgroup_width_avg(int64_t f, int64_t na, int G) {
   int64_t avg = na > 0 ? f / na : 0;
   int S = avg >= 24 ? 32 : avg >= 12 ? 16 : avg >= 6 ? 8 : avg >= 3 ? 4 : 2;

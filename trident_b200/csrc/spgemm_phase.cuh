@@ -46,27 +46,9 @@ __device__ __forceinline__ void walk_row(const int32_t *__restrict__ Bj,
   }
 }
 
-// Product loop: sub-groups of S threads take A entries in turn; the S threads
-// of a sub-group stride over that entry's B row.  f(col, a*b) per product.
-template <int G, bool NUM, typename PT, typename VT, typename F>
-__device__ __forceinline__ void for_products(const int32_t *__restrict__ Aj,
-                                             const VT *__restrict__ Ax,
-                                             const PT *__restrict__ Bp,
-                                             const int32_t *__restrict__ Bj,
-                                             const VT *__restrict__ Bx,
-                                             int64_t a0, int64_t a1, int S,
-                                             int lane, F &&f) {
-  const int sub = lane / S, sl = lane - sub * S, nsub = G / S;
-  for (int64_t p = a0 + sub; p < a1; p += nsub) {
-    const int64_t k = __ldg(Aj + p);
-    VT a = VT(0);
-    if constexpr (NUM) a = __ldg(Ax + p);
-    walk_row<NUM, VT>(Bj, Bx, __ldg(Bp + k) + sl, __ldg(Bp + k + 1), S, a, f);
-  }
-}
-
-// Balanced product loop for one row by a group of G threads.  Pass 1: as
-// for_products, but an A entry whose B row is longer than the fair share of a
+// Balanced product loop for one row by a group of G threads.  Pass 1:
+// sub-groups of S threads take A entries in turn and stride over the entry's
+// B row, but an A entry whose B row is longer than the fair share of a
 // sub-group (f / #sub-groups) is appended to `lst` (group-private shared
 // memory, `cap` slots, count in *nl) instead; pass 2 walks each listed B row
 // with all G threads, so a hub row of B never leaves the group waiting on
