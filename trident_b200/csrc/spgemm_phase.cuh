@@ -52,33 +52,47 @@ __device__ __forceinline__ void walk_row(const int32_t *__restrict__ Bj,
 // sub-group (f / #sub-groups) is appended to `lst` (group-private shared
 // memory, `cap` slots, count in *nl) instead; pass 2 walks each listed B row
 // with all G threads, so a hub row of B never leaves the group waiting on
-// one warp.  When the list is full the entry is done in pass 1.
+// one warp.  When the list is full the entry is done in pass 1.  With `ctr`
+// (a group-private shared int) sub-groups take their next A entry from it as
+// they finish instead of a fixed stride, so uneven B rows do not leave most of
+// the group waiting at the pass's closing barrier.
 template <int G, bool NUM, typename PT, typename VT, typename F>
 __device__ __forceinline__ void for_products_balanced(
     const int32_t *__restrict__ Aj, const VT *__restrict__ Ax,
     const PT *__restrict__ Bp, const int32_t *__restrict__ Bj,
     const VT *__restrict__ Bx, int64_t a0, int64_t a1, int64_t f, int S,
-    int lane, int gid, int *lst, int *nl, int cap, F &&fn) {
+    int lane, int gid, int *lst, int *nl, int cap, F &&fn, int *ctr = nullptr) {
   const int sub = lane / S, sl = lane - sub * S, nsub = G / S;
   const int64_t thr = nsub > 1 ? max(int64_t(4 * S), f / nsub) : INT64_MAX;
   const unsigned submask =
       S >= 32 ? 0xffffffffu : (((1u << S) - 1u) << (((lane & 31) / S) * S));
-  if (lane == 0) *nl = 0;
+  if (lane == 0) {
+    *nl = 0;
+    if (ctr) *ctr = nsub;
+  }
   group_sync<G>(gid);
-  for (int64_t p = a0 + sub; p < a1; p += nsub) {
-    const int64_t k = __ldg(Aj + p);
+  for (int64_t p = a0 + sub; p < a1;) {
+    const int64_t pc = p;
+    if (ctr) {  // the next entry for this sub-group (dynamic)
+      int t = 0;
+      if (sl == 0) t = atomicAdd(ctr, 1);
+      p = a0 + __shfl_sync(submask, t, (lane & 31) - sl);
+    } else {
+      p += nsub;
+    }
+    const int64_t k = __ldg(Aj + pc);
     const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
     if (b1 - b0 > thr) {
       int slot = 0;
       if (sl == 0) slot = atomicAdd(nl, 1);
       slot = __shfl_sync(submask, slot, (lane & 31) - sl);
       if (slot < cap) {
-        if (sl == 0) lst[slot] = int(p - a0);
+        if (sl == 0) lst[slot] = int(pc - a0);
         continue;
       }
     }
     VT a = VT(0);
-    if constexpr (NUM) a = __ldg(Ax + p);
+    if constexpr (NUM) a = __ldg(Ax + pc);
     walk_row<NUM, VT>(Bj, Bx, b0 + sl, b1, S, a, fn);
   }
   group_sync<G>(gid);
@@ -362,7 +376,7 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     };
     for_products_balanced<kThreads, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
                                                    A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl,
-                                                   gm.cap, mark);
+                                                   gm.cap, mark, gm.nl - 1);
     for_addend<false>(P, rr.r, tid, kThreads, mark);
     __syncthreads();
     int64_t local = 0;
@@ -799,7 +813,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     if (!(*(volatile uint32_t *)&x & bit)) atomicOr(&x, bit);
   };
   for_products_balanced<kThreads, false, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
-                                                 gm.lst, gm.nl, gm.cap, mark);
+                                                 gm.lst, gm.nl, gm.cap, mark, gm.nl - 1);
   for_addend<false>(P, rr.r, tid, kThreads, mark);
   __syncthreads();
   prof_sub(A, 0, tp);
@@ -913,7 +927,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   };
   auto put = [&](int32_t col, VT v) { red_add_hint(Cx + rank_of(col), v, keep); };
   for_products_balanced<kThreads, true, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
-                                                gm.lst, gm.nl, gm.cap, put);
+                                                gm.lst, gm.nl, gm.cap, put, gm.nl - 1);
   for_addend<true>(P, rr.r, tid, kThreads, put);
   __syncthreads();
   prof_sub(A, 4, tp);
@@ -1100,7 +1114,7 @@ struct PhaseShared {
   int lst[1024];              // deferred long B rows: CTA 1024, 256-group g at 256g,
                               // 128-group g at 128g, warp w at 32w
   int nl[48];                 // list counts: 256-groups 0-3, 128-groups 4-11,
-                              // warps 12-43, CTA 47
+                              // warps 12-43, CTA 47; [46] the CTA's entry counter
   int64_t off[NCLS], cnt[NCLS];
 };
 
