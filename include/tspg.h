@@ -309,18 +309,24 @@ int tspg_batch_add(tspg_batch *b, const tspg_csr *A, const tspg_csr *B,
 /* Runs all products; synchronises `stream` once (for the output size). */
 int tspg_batch_run(tspg_batch *b, void *stream, int flags,
                    int64_t *total_nnz);
+/* The flop-count pass of tspg_spgemm_count for every product of the batch in
+ * one launch: mults[i] and c_nnz_upper[i] for product i (arrays of the
+ * batch's size).  Synchronises `stream` once; does not run the products. */
+int tspg_batch_count(tspg_batch *b, void *stream, int64_t *mults,
+                     int64_t *c_nnz_upper);
 /* View of result i (device pointers into the batch's slab, int64 rowptr). */
 int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out);
 
 /* ---- serving ---------------------------------------------------------------------
  * A continuous-batching server for C = A·B and Galerkin C = R·(A·P) requests
  * with device-resident operands (borrowed until the request completes).
- * Every request is admitted against `mem_budget` bytes by the upper bound on
- * its output from the flop-count pass; admitted requests wait in a FIFO, and
- * each of `lanes` worker threads (own context and stream) takes all waiting
- * requests (up to max_batch) whenever it frees up and runs them as one
- * batched product per stage, so batches formed while others run overlap on
- * the device.  Results (int64 row offsets) stay valid until release. */
+ * Requests wait in a FIFO; each of `lanes` worker threads (own context and
+ * stream) takes the waiting requests (up to max_batch) whenever it frees up,
+ * bounds their outputs with one batched flop-count pass, admits the FIFO
+ * prefix that fits `mem_budget` bytes (the rest go back to the head of the
+ * queue) and runs it as one batched product per stage, so batches formed
+ * while others run overlap on the device.  Submission does no device work.
+ * Results (int64 row offsets) stay valid until release. */
 enum { TSPG_REQ_AB = 0, TSPG_REQ_RAP = 1 };
 typedef struct tspg_server tspg_server;
 typedef struct tspg_server_config {
@@ -334,8 +340,9 @@ int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
                        tspg_server **out);
 int tspg_server_destroy(tspg_server *s);
 /* kind TSPG_REQ_AB: C = A·B (R unused); TSPG_REQ_RAP: C = R·(A·B) with B the
- * prolongator.  Returns TSPG_ENOMEM when the request alone exceeds the
- * budget.  Thread-safe. */
+ * prolongator.  Checks the shapes and enqueues; a request whose output bound
+ * alone exceeds the budget completes with TSPG_ENOMEM (from
+ * tspg_server_wait).  Thread-safe. */
 int tspg_server_submit(tspg_server *s, int kind, const tspg_csr *A,
                        const tspg_csr *B, const tspg_csr *R, int64_t *ticket);
 /* Wait up to timeout_ms (< 0: forever) for a ticket; TSPG_ETIMEOUT if not

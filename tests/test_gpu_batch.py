@@ -100,3 +100,30 @@ def test_batch_reuse_grows_rows_not_nnz(ctx):
     check_product(b.result(0), A2, A2)
     check_product(b.result(1), A1, A1)
     b.close()
+
+
+def test_batch_count_matches_oracle(ctx):
+    # per-product flop counts of one launch, mixed offset widths, empty
+    # products and long rows among short ones
+    from trident_b200.csr import HostCSR
+    import oracle
+    E = HostCSR(0, 5, np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0))
+    B5 = random_csr(5, 9, density=0.5, seed=1)
+    pairs = [(workloads.poisson_rows(3000, 12.0, 3), workloads.poisson_rows(3000, 12.0, 4), 32, 64),
+             (E, B5, 64, 64),
+             (random_csr(40, 3000, per_row=900, seed=5), random_csr(3000, 700, per_row=20, seed=6), 64, 32),
+             (workloads.rmat(scale=10, edge_factor=16, seed=7), None, 32, 32)]
+    b = ops.Batch(ctx)
+    keep = []
+    for A, B, ra, rb in pairs:
+        B = A if B is None else B
+        dA, dB = A.to_device(rowptr_bits=ra), B.to_device(rowptr_bits=rb)
+        keep.append((A, B, dA, dB))
+        b.add(dA, dB)
+    got = b.count()
+    for (A, B, dA, dB), (m, u) in zip(keep, got):
+        rm = oracle.row_mults(A, B)
+        assert m == int(rm.sum())
+        assert u == int(np.minimum(rm, B.ncols).sum())
+        assert (m, u) == ops.spgemm_count(ctx, dA, dB)
+    b.close()

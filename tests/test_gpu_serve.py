@@ -6,7 +6,7 @@ import threading
 import numpy as np
 import pytest
 
-from helpers import TOL64
+from helpers import TOL64, random_csr
 from trident_b200 import ops, workloads
 
 pytestmark = pytest.mark.gpu
@@ -59,10 +59,37 @@ def test_server_mix_matches_alone(ctx):
 
 
 def test_server_rejects_oversized_request(ctx):
-    A = workloads.poisson_rows(5000, 20.0, 2).to_device()
+    # the bound of the first request alone exceeds the budget: it completes
+    # with ENOMEM; the small one behind it still runs
+    A = workloads.poisson_rows(5000, 20.0, 2)
+    S = workloads.poisson_rows(50, 2.0, 3)
+    dA, dS = A.to_device(), S.to_device()
     srv = ops.Server(ctx, mem_budget=1 << 20, lanes=1, max_batch=4)
     from trident_b200._lib import TSPG_ENOMEM, TspgError
+    t_big, t_small = srv.submit(dA, dA), srv.submit(dS, dS)
     with pytest.raises(TspgError) as e:
-        srv.submit(A, A)
+        srv.wait(t_big, timeout_ms=60000)
     assert e.value.status == TSPG_ENOMEM
+    srv.release(t_big)
+    res, _ = srv.wait(t_small, timeout_ms=60000)
+    _same(res.to_host(), ops.spgemm(ctx, dS, dS).to_host())
+    srv.release(t_small)
+    st = srv.stats()
+    assert st["completed"] == 1 and st["reserved"] == 0
+    srv.close()
+
+
+def test_server_refuses_bad_shapes(ctx):
+    A = workloads.poisson_rows(300, 4.0, 4).to_device()
+    B = random_csr(200, 300, density=0.02, seed=5).to_device()
+    srv = ops.Server(ctx, mem_budget=1 << 30, lanes=1, max_batch=4)
+    from trident_b200._lib import TSPG_EINVAL, TspgError
+    with pytest.raises(TspgError) as e:
+        srv.submit(A, B)  # 300 columns against 200 rows
+    assert e.value.status == TSPG_EINVAL
+    R = random_csr(10, 200, density=0.1, seed=6).to_device()
+    with pytest.raises(TspgError) as e:
+        srv.submit(A, A, R)  # R has 200 columns against A's 300 rows
+    assert e.value.status == TSPG_EINVAL
+    assert srv.stats()["queued"] == 0
     srv.close()

@@ -112,6 +112,7 @@ def _load() -> C.CDLL:
         "tspg_batch_clear": (i32, [vp]),
         "tspg_batch_add": (i32, [vp, P(TspgCsr), P(TspgCsr), P(C.c_int)]),
         "tspg_batch_run": (i32, [vp, vp, i32, P(i64)]),
+        "tspg_batch_count": (i32, [vp, vp, P(i64), P(i64)]),
         "tspg_batch_result": (i32, [vp, i32, P(TspgCsr)]),
         "tspg_spgemm_count": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(i64), P(i64)]),
         "tspg_spgemm": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(TspgCsrOut), i32]),

@@ -63,6 +63,58 @@ __global__ void k_set_batch_out(ProdDev<PT, VT> *prods, const int64_t *base,
   }
 }
 
+// Operands of one product for the batched flop-count pass (either offset width).
+struct CountDesc {
+  const void *Ap;
+  const int32_t *Aj;
+  const void *Bp;
+  int64_t n;
+  int a64, b64;
+};
+
+// Flop count and output upper bound of every product of a batch in one launch:
+// one thread per row of the flat row space (rows of a product are contiguous,
+// so the products of a warp's 32 rows are non-decreasing over its lanes), a
+// segmented inclusive warp sum per product and one 64-bit atomic per segment.
+// out[2p] = sum of products, out[2p + 1] = sum over rows of min(products, ncols).
+__global__ void k_count_batch(const CountDesc *d, const int64_t *base, int nprod, int64_t R,
+                              unsigned long long *out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t w0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x - lane; w0 < R; w0 += stride) {
+    const int64_t g = w0 + lane;
+    int p = -1;
+    long long mu = 0, up = 0;
+    if (g < R) {
+      p = find_prod(base, nprod, g);
+      const int64_t r = g - base[p];
+      const CountDesc c = d[p];
+      const int64_t a0 = c.a64 ? ((const int64_t *)c.Ap)[r] : ((const int32_t *)c.Ap)[r];
+      const int64_t a1 = c.a64 ? ((const int64_t *)c.Ap)[r + 1] : ((const int32_t *)c.Ap)[r + 1];
+      for (int64_t q = a0; q < a1; ++q) {
+        const int32_t k = __ldg(c.Aj + q);
+        mu += c.b64 ? ((const int64_t *)c.Bp)[k + 1] - ((const int64_t *)c.Bp)[k]
+                    : ((const int32_t *)c.Bp)[k + 1] - ((const int32_t *)c.Bp)[k];
+      }
+      up = mu < c.n ? mu : c.n;
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long m2 = __shfl_up_sync(0xffffffffu, mu, o);
+      const long long u2 = __shfl_up_sync(0xffffffffu, up, o);
+      const int p2 = __shfl_up_sync(0xffffffffu, p, o);
+      if (lane >= o && p2 == p) {
+        mu += m2;
+        up += u2;
+      }
+    }
+    const int pn = __shfl_down_sync(0xffffffffu, p, 1);
+    if (p >= 0 && (lane == 31 || pn != p)) {
+      atomicAdd(out + 2 * p, (unsigned long long)mu);
+      atomicAdd(out + 2 * p + 1, (unsigned long long)up);
+    }
+  }
+}
+
 }  // namespace tspg
 
 using namespace tspg;
@@ -94,6 +146,8 @@ struct tspg_batch {
   int64_t cap_rows = 0, cap_nnz = 0, cap_cur = 0, cap_prod = 0;
   int64_t *h_offs = nullptr;  // pinned, cap_prod + 1
   size_t h_offs_cap = 0;
+  int64_t *h_cnt = nullptr;  // pinned, 2 per product (tspg_batch_count)
+  size_t h_cnt_cap = 0;
   cudaGraphExec_t g1 = nullptr, g2 = nullptr;
   // graphs are captured and launched on a batch-private stream (capture is
   // not allowed on the legacy default stream); events join it to the caller's
@@ -396,6 +450,7 @@ extern "C" int tspg_batch_destroy(tspg_batch *b) {
   b->drop_graphs();
   b->free_dev(nullptr);
   if (b->h_offs) cudaFreeHost(b->h_offs);
+  if (b->h_cnt) cudaFreeHost(b->h_cnt);
   if (b->join_in) cudaEventDestroy(b->join_in);
   if (b->join_out) cudaEventDestroy(b->join_out);
   if (b->own) cudaStreamDestroy(b->own);
@@ -446,6 +501,57 @@ extern "C" int tspg_batch_run(tspg_batch *b, void *stream, int flags, int64_t *t
   else st = batch_run_joined<int64_t, float>(b, s, flags);
   if (st == TSPG_OK && total_nnz) *total_nnz = b->total_nnz;
   return st;
+}
+
+extern "C" int tspg_batch_count(tspg_batch *b, void *stream, int64_t *mults,
+                                int64_t *c_nnz_upper) {
+  if (!b) return TSPG_EINVAL;
+  const int nprod = (int)b->A.size();
+  if (nprod == 0) return TSPG_OK;
+  if (!mults || !c_nnz_upper) return TSPG_EINVAL;
+  tspg_ctx *ctx = b->ctx;
+  TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<CountDesc> hd(nprod);
+  std::vector<int64_t> base(nprod + 1, 0);
+  for (int p = 0; p < nprod; ++p) {
+    hd[p] = CountDesc{b->A[p].rowptr, b->A[p].col, b->B[p].rowptr, b->B[p].ncols,
+                      b->A[p].rowptr_bits == 64, b->B[p].rowptr_bits == 64};
+    base[p + 1] = base[p] + b->A[p].nrows;
+  }
+  const int64_t R = base[nprod];
+  if (size_t(2 * nprod) > b->h_cnt_cap) {
+    if (b->h_cnt) cudaFreeHost(b->h_cnt);
+    b->h_cnt = nullptr;
+    b->h_cnt_cap = 0;
+    TSPG_CUDA(ctx, cudaMallocHost((void **)&b->h_cnt, sizeof(int64_t) * 2 * nprod));
+    b->h_cnt_cap = 2 * nprod;
+  }
+  Scratch sc(ctx, s);
+  CountDesc *dd;
+  int64_t *dbase;
+  unsigned long long *dout;
+  TSPG_TRY(sc.get(&dd, nprod));
+  TSPG_TRY(sc.get(&dbase, nprod + 1));
+  TSPG_TRY(sc.get(&dout, 2 * nprod));
+  // pageable sources: staged before the calls return
+  TSPG_CUDA(ctx, cudaMemcpyAsync(dd, hd.data(), sizeof(CountDesc) * nprod, cudaMemcpyHostToDevice, s));
+  TSPG_CUDA(ctx, cudaMemcpyAsync(dbase, base.data(), sizeof(int64_t) * (nprod + 1),
+                                 cudaMemcpyHostToDevice, s));
+  TSPG_CUDA(ctx, cudaMemsetAsync(dout, 0, sizeof(int64_t) * 2 * nprod, s));
+  if (R > 0) {
+    k_count_batch<<<(unsigned)std::min<int64_t>((R + 255) / 256, int64_t(ctx->num_sms) * 8), 256, 0,
+                    s>>>(dd, dbase, nprod, R, dout);
+    ctx->launches += 1;
+    TSPG_CUDA(ctx, cudaGetLastError());
+  }
+  TSPG_CUDA(ctx, cudaMemcpyAsync(b->h_cnt, dout, sizeof(int64_t) * 2 * nprod, cudaMemcpyDeviceToHost, s));
+  TSPG_CUDA(ctx, cudaStreamSynchronize(s));
+  for (int p = 0; p < nprod; ++p) {
+    mults[p] = b->h_cnt[2 * p];
+    c_nnz_upper[p] = b->h_cnt[2 * p + 1];
+  }
+  return TSPG_OK;
 }
 
 extern "C" int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out) {

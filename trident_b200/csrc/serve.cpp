@@ -1,17 +1,18 @@
 // serve.cpp — continuous-batching server for A·B and Galerkin R·A·P requests.
 //
 // Requests arrive on any host thread (tspg_server_submit) with device-resident
-// operands.  Each is admitted against a device-memory budget by the upper
-// bound on its output from the flop-count pass (sum_i min(mults_i, ncols), 12
-// bytes per entry plus row offsets); requests wait in a FIFO until the budget
-// allows.  `lanes` worker threads, each with its own context, stream and two
-// tspg_batch objects, take every admitted request that is waiting when the
-// lane frees up (up to max_batch) and run them as one batched product per
-// stage: stage 1 = all A·B requests plus the A·P half of the R·A·P requests,
-// stage 2 = R·(AP) for the R·A·P requests.  Lanes run concurrently on their
-// own streams, so a batch that forms while others are on the GPU overlaps
-// with them.  Results are copied out of the batch slab into per-request
-// buffers from the lane's pool, which stay valid until tspg_server_release.
+// operands and wait in a FIFO; submission does no device work.  `lanes` worker
+// threads, each with its own context, stream and tspg_batch objects, take the
+// waiting requests (up to max_batch) when the lane frees up, bound every
+// output with one batched flop-count pass (sum_i min(mults_i, ncols), 12 bytes
+// per entry plus row offsets), admit the FIFO prefix that fits the device-
+// memory budget and put the rest back at the head of the queue.  The admitted
+// requests run as one batched product per stage: stage 1 = all A·B requests
+// plus the A·P half of the R·A·P requests, stage 2 = R·(AP) for the R·A·P
+// requests.  Lanes run concurrently on their own streams, so a batch that
+// forms while others are on the device overlaps with them.  Results are copied
+// out of the batch slab into per-request buffers from the lane's pool, which
+// stay valid until tspg_server_release.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -26,6 +27,12 @@
 #include <cuda_runtime.h>
 
 #include "tspg.h"
+
+#define TSPG_TRY_HOST(x)        \
+  do {                          \
+    const int st_ = (x);        \
+    if (st_ != TSPG_OK) return st_; \
+  } while (0)
 
 namespace tspg {
 int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
@@ -43,7 +50,9 @@ struct Req {
   int64_t ticket = 0;
   int kind = TSPG_REQ_AB;
   tspg_csr A{}, B{}, R{};
-  size_t reserve = 0;  // admitted bytes
+  size_t reserve = 0;  // output bound (bytes), reserved while admitted
+  bool bounded = false;
+  bool admitted = false;
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = TSPG_OK;
   bool done = false;
@@ -60,8 +69,6 @@ struct Req {
 struct tspg_server {
   int device = 0;
   tspg_server_config cfg{};
-  tspg_ctx *adm = nullptr;  // admission context (count pass), used under mu
-  cudaStream_t adm_stream = nullptr;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Req *> queue;
@@ -77,6 +84,16 @@ struct tspg_server {
 };
 
 namespace {
+
+// The operand checks of the product entry points, on the host.
+bool csr_ok(const tspg_csr *M) {
+  if (M->nrows < 0 || M->ncols < 0 || M->nnz < 0 || M->ncols > INT32_MAX) return false;
+  if ((M->rowptr_bits != 32 && M->rowptr_bits != 64) || (M->val_bits != 32 && M->val_bits != 64))
+    return false;
+  if (M->rowptr_bits == 32 && M->nnz > INT32_MAX) return false;
+  if (M->nnz > 0 && (!M->col || !M->val)) return false;
+  return M->rowptr || M->nrows == 0;
+}
 
 size_t out_bytes(int64_t nnz_upper, int64_t rows, int vb) {
   return size_t(nnz_upper) * size_t(4 + vb) + size_t(rows + 1) * 8;
@@ -108,36 +125,101 @@ int take_result(tspg_ctx *ctx, cudaStream_t s, tspg_batch *b, int i, Req *r, int
   return TSPG_OK;
 }
 
+// Output bounds (bytes) of the requests not bounded yet, one batched count
+// pass: the A·B output, or A·P plus R·A·P (bounded by rows(R) x ncols(P)) for
+// the Galerkin product.
+int bound_requests(tspg_batch *bc, cudaStream_t s, const std::vector<Req *> &cand) {
+  std::vector<Req *> todo;
+  tspg_batch_clear(bc);
+  for (Req *r : cand) {
+    if (r->bounded) continue;
+    int idx = 0;
+    TSPG_TRY_HOST(tspg_batch_add(bc, &r->A, &r->B, &idx));
+    todo.push_back(r);
+  }
+  if (todo.empty()) return TSPG_OK;
+  std::vector<int64_t> mults(todo.size()), upper(todo.size());
+  TSPG_TRY_HOST(tspg_batch_count(bc, s, mults.data(), upper.data()));
+  for (size_t i = 0; i < todo.size(); ++i) {
+    Req *r = todo[i];
+    const int vb = r->A.val_bits / 8;
+    size_t bytes = out_bytes(upper[i], r->A.nrows, vb);
+    if (r->kind == TSPG_REQ_RAP) {
+      const int64_t full = r->R.nrows * r->B.ncols;
+      const int64_t up2 = std::min<int64_t>(
+          full, upper[i] > 0 ? r->R.nnz * (upper[i] / std::max<int64_t>(1, r->A.nrows) + 1) : 0);
+      bytes += out_bytes(up2, r->R.nrows, vb);
+    }
+    r->reserve = bytes;
+    r->bounded = true;
+  }
+  return TSPG_OK;
+}
+
 void lane_main(tspg_server *S, int lane) {
   cudaSetDevice(S->device);
   tspg_ctx *ctx = S->lane_ctx[lane];
   cudaStream_t s = S->lane_stream[lane];
-  tspg_batch *b1 = nullptr, *b2 = nullptr;
+  tspg_batch *b1 = nullptr, *b2 = nullptr, *bc = nullptr;
   tspg_batch_create(ctx, &b1);
   tspg_batch_create(ctx, &b2);
-  std::vector<Req *> take;
+  tspg_batch_create(ctx, &bc);
+  std::vector<Req *> cand, take, back;
   while (true) {
+    cand.clear();
     take.clear();
+    back.clear();
     {
       std::unique_lock<std::mutex> lk(S->mu);
       S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
       if (S->stop && S->queue.empty()) break;
-      // FIFO admission by the memory budget; the head request is always
-      // admitted when nothing else is reserved (it was checked to fit alone)
-      while (!S->queue.empty() && (int)take.size() < S->cfg.max_batch) {
-        Req *r = S->queue.front();
-        if (S->reserved + r->reserve > S->cfg.mem_budget && !(S->reserved == 0 && take.empty()))
-          break;
+      // claim the head of the queue (one value width per batch)
+      while (!S->queue.empty() && (int)cand.size() < S->cfg.max_batch &&
+             (cand.empty() || S->queue.front()->A.val_bits == cand[0]->A.val_bits)) {
+        cand.push_back(S->queue.front());
         S->queue.pop_front();
-        S->reserved += r->reserve;
-        take.push_back(r);
       }
+    }
+    const int bst = bound_requests(bc, s, cand);
+    bool rejected = false;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      // FIFO admission by the memory budget; the head request is admitted
+      // whenever nothing else is reserved, unless it exceeds the budget alone
+      for (Req *r : cand) {
+        const bool fail = bst != TSPG_OK || r->reserve > S->cfg.mem_budget;
+        if (fail) {
+          r->status = bst != TSPG_OK ? bst : TSPG_ENOMEM;
+          r->t_done = now_ms();
+          r->done = true;
+          S->rejected += 1;
+          rejected = true;
+          continue;
+        }
+        if (back.empty() && (S->reserved + r->reserve <= S->cfg.mem_budget ||
+                             (S->reserved == 0 && take.empty()))) {
+          S->reserved += r->reserve;
+          r->admitted = true;
+          take.push_back(r);
+        } else {
+          back.push_back(r);
+        }
+      }
+      for (auto it = back.rbegin(); it != back.rend(); ++it) S->queue.push_front(*it);
+      if (bst != TSPG_OK) S->lane_error = bst;
       if (take.empty()) {
+        if (rejected) {
+          lk.unlock();
+          S->cv_done.notify_all();
+          continue;
+        }
         // budget held by other lanes: wait for a release
         S->cv_done.wait_for(lk, std::chrono::milliseconds(1));
         continue;
       }
     }
+    if (rejected) S->cv_done.notify_all();
+    if (!back.empty()) S->cv_work.notify_one();
     const double t0 = now_ms();
     for (Req *r : take) r->t_start = t0;
     int st = TSPG_OK;
@@ -182,7 +264,7 @@ void lane_main(tspg_server *S, int lane) {
         r->done = true;
         if (st != TSPG_OK) {
           S->reserved -= r->reserve;
-          r->reserve = 0;
+          r->admitted = false;
         }
       }
       S->batches += 1;
@@ -193,6 +275,7 @@ void lane_main(tspg_server *S, int lane) {
   }
   tspg_batch_destroy(b1);
   tspg_batch_destroy(b2);
+  tspg_batch_destroy(bc);
 }
 
 }  // namespace
@@ -209,11 +292,8 @@ extern "C" int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
   int dev = 0;
   cudaGetDevice(&dev);
   S->device = dev;
-  int st = tspg_ctx_create(dev, 0, &S->adm);
-  if (st == TSPG_OK && cudaStreamCreateWithFlags(&S->adm_stream, cudaStreamNonBlocking) != cudaSuccess)
-    st = TSPG_ECUDA;
   tspg_tuning tune;  // lanes take the row binning of the parent context
-  if (st == TSPG_OK) st = tspg_ctx_get_tuning(ctx, &tune);
+  int st = tspg_ctx_get_tuning(ctx, &tune);
   for (int l = 0; l < cfg->lanes && st == TSPG_OK; ++l) {
     tspg_ctx *c = nullptr;
     cudaStream_t ls = nullptr;
@@ -258,8 +338,6 @@ extern "C" int tspg_server_destroy(tspg_server *S) {
     if (S->lane_stream[l]) cudaStreamDestroy(S->lane_stream[l]);
     if (S->lane_ctx[l]) tspg_ctx_destroy(S->lane_ctx[l]);
   }
-  if (S->adm_stream) cudaStreamDestroy(S->adm_stream);
-  if (S->adm) tspg_ctx_destroy(S->adm);
   delete S;
   return TSPG_OK;
 }
@@ -269,6 +347,11 @@ extern "C" int tspg_server_submit(tspg_server *S, int kind, const tspg_csr *A,
   if (!S || !A || !B || !ticket) return TSPG_EINVAL;
   if (kind != TSPG_REQ_AB && kind != TSPG_REQ_RAP) return TSPG_EINVAL;
   if (kind == TSPG_REQ_RAP && !R) return TSPG_EINVAL;
+  if (!csr_ok(A) || !csr_ok(B) || A->ncols != B->nrows || A->val_bits != B->val_bits)
+    return TSPG_EINVAL;
+  if (kind == TSPG_REQ_RAP &&
+      (!csr_ok(R) || R->ncols != A->nrows || R->val_bits != A->val_bits))
+    return TSPG_EINVAL;
   Req *r = new (std::nothrow) Req();
   if (!r) return TSPG_ENOMEM;
   r->kind = kind;
@@ -277,28 +360,6 @@ extern "C" int tspg_server_submit(tspg_server *S, int kind, const tspg_csr *A,
   if (R) r->R = *R;
   r->t_submit = now_ms();
   std::lock_guard<std::mutex> lk(S->mu);
-  // admission bound from the count pass: the A·B output, or A·P plus R·A·P
-  // (bounded by rows(R) x ncols(P)) for the Galerkin product
-  int64_t mults = 0, upper = 0;
-  cudaSetDevice(S->device);
-  int st = tspg_spgemm_count(S->adm, S->adm_stream, A, B, &mults, &upper);
-  if (st != TSPG_OK) {
-    delete r;
-    return st;
-  }
-  const int vb = A->val_bits / 8;
-  size_t bytes = out_bytes(upper, A->nrows, vb);
-  if (kind == TSPG_REQ_RAP) {
-    const int64_t full = R->nrows * B->ncols;
-    const int64_t up2 = std::min<int64_t>(full, upper > 0 ? R->nnz * (upper / std::max<int64_t>(1, A->nrows) + 1) : 0);
-    bytes += out_bytes(up2, R->nrows, vb);
-  }
-  r->reserve = bytes;
-  if (bytes > S->cfg.mem_budget) {
-    delete r;
-    S->rejected += 1;
-    return TSPG_ENOMEM;
-  }
   r->ticket = S->next_ticket++;
   S->reqs[r->ticket] = r;
   S->queue.push_back(r);
@@ -347,7 +408,7 @@ extern "C" int tspg_server_release(tspg_server *S, int64_t ticket) {
     if (it == S->reqs.end() || !it->second->done) return TSPG_EINVAL;
     r = it->second;
     S->reqs.erase(it);
-    S->reserved -= r->reserve;
+    if (r->admitted) S->reserved -= r->reserve;
   }
   if (r->lane >= 0) {
     // the lane's pool is stream-ordered on the lane stream; its work on these

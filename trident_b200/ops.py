@@ -306,6 +306,13 @@ class Batch:
         check(lib.tspg_batch_run(self.h, _stream_ptr(stream), flags, C.byref(tot)), "tspg_batch_run")
         return tot.value
 
+    def count(self, stream=None) -> list[tuple[int, int]]:
+        """(mults, sum_i min(mults_i, ncols)) of every product, one launch."""
+        n = len(self._keep)
+        mults, up = (C.c_int64 * max(n, 1))(), (C.c_int64 * max(n, 1))()
+        check(lib.tspg_batch_count(self.h, _stream_ptr(stream), mults, up), "tspg_batch_count")
+        return [(mults[i], up[i]) for i in range(n)]
+
     def result(self, i: int) -> DeviceCSR:
         """Result i as a DeviceCSR whose tensors alias the batch's output slab."""
         v = TspgCsr()
