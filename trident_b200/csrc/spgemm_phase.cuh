@@ -299,6 +299,47 @@ __device__ __forceinline__ RowRef decode_row(const PhaseArgs &A, int64_t idx) {
   return rr;
 }
 
+// What a group row function needs before its first product: the product, the
+// local and flat row, its product count f, output count c and output offset
+// inside the product (numeric phase only), and its A row bounds.  A chain of
+// three dependent global loads, so warps fetch a whole chunk of rows' metadata
+// at once (one row per lane) and pass it on by shuffles.
+struct RowMeta {
+  int p;
+  int64_t r, g, f, c, off, a0, a1;
+};
+
+template <bool NUM, typename PT, typename VT>
+__device__ __forceinline__ RowMeta load_meta(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                                             int64_t idx) {
+  const uint64_t e = A.list[idx];
+  RowMeta m;
+  m.p = int(e >> 40);
+  m.r = int64_t(e & ((uint64_t(1) << 40) - 1));
+  const int64_t b = A.base[m.p];
+  const PT *Ap = prods[m.p].Ap;
+  m.g = b + m.r;
+  m.a0 = int64_t(Ap[m.r]);
+  m.a1 = int64_t(Ap[m.r + 1]);
+  m.f = A.rowf[m.g];
+  m.c = NUM ? int64_t(A.rowc[m.g]) : 0;
+  m.off = NUM ? A.cp[m.g] - A.cp[b] : 0;
+  return m;
+}
+
+__device__ __forceinline__ RowMeta shfl_meta(const RowMeta &m, int src) {
+  RowMeta o;
+  o.p = __shfl_sync(0xffffffffu, m.p, src);
+  o.r = __shfl_sync(0xffffffffu, m.r, src);
+  o.g = __shfl_sync(0xffffffffu, m.g, src);
+  o.f = __shfl_sync(0xffffffffu, m.f, src);
+  o.c = __shfl_sync(0xffffffffu, m.c, src);
+  o.off = __shfl_sync(0xffffffffu, m.off, src);
+  o.a0 = __shfl_sync(0xffffffffu, m.a0, src);
+  o.a1 = __shfl_sync(0xffffffffu, m.a1, src);
+  return o;
+}
+
 // Group-private shared scratch handed to the row functions.
 struct GroupMem {
   int64_t *tmp;   // scan scratch (33 words)
@@ -310,25 +351,37 @@ struct GroupMem {
   unsigned char *stage;  // flat product loop staging (G = 128 / 256), 24 B per lane
 };
 
+// Hash table clears with 16-byte shared stores (T is a power of two >= 32 and
+// every table starts on a 16-byte boundary of its slice).
+template <int G>
+__device__ __forceinline__ void clear_keys(int *keys, uint32_t T, int lane) {
+  int4 *k4 = reinterpret_cast<int4 *>(keys);
+  for (uint32_t s = lane; s < T / 4; s += G) k4[s] = make_int4(-1, -1, -1, -1);
+}
+template <int G, typename VT>
+__device__ __forceinline__ void clear_vals(VT *vals, uint32_t T, int lane) {
+  uint4 *v4 = reinterpret_cast<uint4 *>(vals);
+  for (uint32_t s = lane; s < T * uint32_t(sizeof(VT)) / 16; s += G) v4[s] = make_uint4(0, 0, 0, 0);
+}
+
 // ---------------------------------------------------------------- symbolic
 
 template <int G, int TMAX, typename PT, typename VT>
 __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
-                             int64_t idx, int *keys, const GroupMem &gm, int gid,
+                             const RowMeta &m, int *keys, const GroupMem &gm, int gid,
                              int lane) {
   long long tp = clock64();
-  const RowRef rr = decode_row(A, idx);
-  const ProdDev<PT, VT> &P = prods[rr.p];
-  const int64_t f = A.rowf[rr.g];
+  const ProdDev<PT, VT> &P = prods[m.p];
+  const int64_t f = m.f;
   const int64_t n = P.n;
   const int64_t fe = f < n ? f : n;
   uint32_t T = pow2_at_least(A.S->tune.load * fe, 32);
   if (T > TMAX) T = TMAX;
   const int logT = ilog2_pow2(T);
   const uint32_t mask = T - 1;
-  for (uint32_t s = lane; s < T; s += G) keys[s] = -1;
+  clear_keys<G>(keys, T, lane);
   group_sync<G>(gid);
-  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int64_t a0 = m.a0, a1 = m.a1;
   prof_sub_g(A, 9, tp, lane == 0);
   int cnt = 0;
   auto ins = [&](int32_t col, VT) { cnt += sym_insert(keys, col, logT, mask, A.err); };
@@ -336,15 +389,15 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     for_products_flat<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
                                         gm.tmp, gm.stage, ins);
   } else {
-    const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
+    const int S = subgroup_width_avg(f, a1 - a0, G);
     for_products_balanced<G, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, f, S, lane,
                                             gid, gm.lst, gm.nl, gm.cap, ins);
   }
-  for_addend<false>(P, rr.r, lane, G, ins);
+  for_addend<false>(P, m.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
   const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
-  if (lane == 0) A.rowc[rr.g] = int32_t(total);
+  if (lane == 0) A.rowc[m.g] = int32_t(total);
   group_sync<G>(gid);
   prof_sub_g(A, 11, tp, lane == 0);
 }
@@ -408,6 +461,27 @@ __device__ __forceinline__ void bitonic_pairs(int *keys, VT *vals, uint32_t P,
         }
       }
       group_sync<G>(gid);
+    }
+  }
+}
+
+// Bitonic sort of one (key, value) pair per lane across a warp, ascending by
+// key, in registers: lanes i < l = i ^ j compare-exchange, the lower lane
+// keeping the smaller key in ascending blocks ((i & k) == 0).  Equal keys stay
+// put, so duplicates survive as adjacent pairs.
+template <typename VT>
+__device__ __forceinline__ void warp_bitonic32(int &key, VT &val, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int pk = __shfl_xor_sync(0xffffffffu, key, j);
+      const VT pv = __shfl_xor_sync(0xffffffffu, val, j);
+      const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
+      if (keep_min ? pk < key : pk > key) {
+        key = pk;
+        val = pv;
+      }
     }
   }
 }
@@ -482,7 +556,7 @@ __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
 
 template <int G, int TMAX, typename PT, typename VT>
 __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
-                             int64_t idx, unsigned char *slice, const GroupMem &gm,
+                             const RowMeta &m, unsigned char *slice, const GroupMem &gm,
                              int gid, int lane) {
   int64_t *tmp = gm.tmp;
   int *itmp = gm.itmp;
@@ -492,20 +566,17 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   VT *vals = (VT *)slice;
   int *keys = (int *)(slice + TMAX * 8);
   long long tp = clock64();
-  const RowRef rr = decode_row(A, idx);
-  const ProdDev<PT, VT> &P = prods[rr.p];
-  const int64_t c = A.rowc[rr.g];
-  const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
+  const ProdDev<PT, VT> &P = prods[m.p];
+  const int64_t c = m.c;
+  const int64_t off = m.off;
   uint32_t T = pow2_at_least(A.S->tune.load * c, 32);
   if (T > TMAX) T = TMAX;
   const int logT = ilog2_pow2(T);
   const uint32_t mask = T - 1;
-  for (uint32_t s = lane; s < T; s += G) {
-    keys[s] = -1;
-    vals[s] = VT(0);
-  }
+  clear_keys<G>(keys, T, lane);
+  clear_vals<G, VT>(vals, T, lane);
   group_sync<G>(gid);
-  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const int64_t a0 = m.a0, a1 = m.a1;
   prof_sub_g(A, 9, tp, lane == 0);
   auto ins = [&](int32_t col, VT v) {
     const uint32_t h = num_insert(keys, col, logT, mask, A.err);
@@ -515,12 +586,11 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     for_products_flat<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
                                        gm.tmp, gm.stage, ins);
   } else {
-    const int S = subgroup_width_avg(A.rowf[rr.g], a1 - a0, G);
-    for_products_balanced<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
-                                           A.rowf[rr.g], S, lane, gid, gm.lst, gm.nl, gm.cap,
-                                           ins);
+    const int S = subgroup_width_avg(m.f, a1 - a0, G);
+    for_products_balanced<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, m.f, S, lane,
+                                           gid, gm.lst, gm.nl, gm.cap, ins);
   }
-  for_addend<true>(P, rr.r, lane, G, ins);
+  for_addend<true>(P, m.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
@@ -579,6 +649,21 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
   group_sync<G>(gid);
   prof_sub_g(A, 11, tp, lane == 0);
+  if constexpr (G == 32) {
+    if (c <= 32) {  // warp rows of up to 32 outputs sort in registers
+      int k = lane < c ? keys[lane] : INT32_MAX;
+      VT v = lane < c ? vals[lane] : VT(0);
+      warp_bitonic32<VT>(k, v, lane);
+      prof_sub_g(A, 12, tp, lane == 0);
+      if (lane < c) {
+        P.Cj[off + lane] = k;
+        P.Cx[off + lane] = v;
+      }
+      __syncwarp();
+      prof_sub_g(A, 13, tp, lane == 0);
+      return;
+    }
+  }
   int src = 0;
   if (!radix) {
     const uint32_t Pw = pow2_at_least(c, 2);
@@ -618,7 +703,7 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 // columns are summed as they are written out.  No hash table to clear, probe
 // or compact; the sort sees f <= 2 c entries instead of c.
 template <int G, int TMAX, typename PT, typename VT>
-__device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, int64_t idx,
+__device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, const RowMeta &m,
                             unsigned char *slice, const GroupMem &gm, int gid, int lane) {
   constexpr int U = 4, FMAX = TMAX / 2, KEEP = TMAX / (2 * G);
   VT *vals = (VT *)slice;  // [0, FMAX) and [FMAX, TMAX): the sort's two buffers
@@ -627,12 +712,11 @@ __device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, in
   int64_t *sb0 = spre + G;
   VT *sa = (VT *)(sb0 + G);
   long long tp = clock64();
-  const RowRef rr = decode_row(A, idx);
-  const ProdDev<PT, VT> &P = prods[rr.p];
-  const int64_t c = A.rowc[rr.g];
-  const int f = int(A.rowf[rr.g]);  // <= FMAX by the caller's test
-  const int64_t off = A.cp[rr.g] - A.cp[A.base[rr.p]];
-  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1];
+  const ProdDev<PT, VT> &P = prods[m.p];
+  const int64_t c = m.c;
+  const int f = int(m.f);  // <= FMAX by the caller's test
+  const int64_t off = m.off;
+  const int64_t a0 = m.a0, a1 = m.a1;
   prof_sub_g(A, 9, tp, lane == 0);
   // expand: every product at its flat index
   int fb = 0;
@@ -703,7 +787,7 @@ __device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, in
   }
   if (P.Ej) {
     int64_t e0, e1;
-    addend_row(P, rr.r, e0, e1);
+    addend_row(P, m.r, e0, e1);
     for (int64_t q = e0 + lane; q < e1; q += G) {
       const int64_t at = fb + (q - e0);
       if (at < FMAX) {
@@ -716,6 +800,36 @@ __device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, in
   group_sync<G>(gid);
   if (lane == 0 && fb != f) set_error(A.err, 107);
   prof_sub_g(A, 10, tp, lane == 0);
+  if constexpr (G == 32) {
+    if (f <= 32) {  // up to 32 products: sort and compress in registers
+      int k = lane < f ? keys[lane] : INT32_MAX;
+      VT v = lane < f ? vals[lane] : VT(0);
+      prof_sub_g(A, 11, tp, lane == 0);
+      warp_bitonic32<VT>(k, v, lane);
+      prof_sub_g(A, 12, tp, lane == 0);
+      // sum each run of equal columns into its first lane (suffix sums inside
+      // runs; keys are sorted, so equal keys are contiguous, and no column
+      // equals the INT32_MAX padding)
+      const int kprev = __shfl_up_sync(0xffffffffu, k, 1);
+      const bool head = lane < f && (lane == 0 || kprev != k);
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int nk = __shfl_down_sync(0xffffffffu, k, o);
+        const VT nv = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o < 32 && nk == k) v += nv;
+      }
+      const unsigned hm = __ballot_sync(0xffffffffu, head);
+      const int pos = __popc(hm & ((1u << lane) - 1u));
+      if (head && pos < c) {
+        P.Cj[off + pos] = k;
+        P.Cx[off + pos] = v;
+      }
+      if (lane == 0 && __popc(hm) != c) set_error(A.err, 108);
+      __syncwarp();
+      prof_sub_g(A, 13, tp, lane == 0);
+      return;
+    }
+  }
   int mn = INT32_MAX, mx = -1;
   for (int e = lane; e < f; e += G) {
     mn = min(mn, keys[e]);
@@ -1121,11 +1235,8 @@ struct PhaseShared {
 // Group rows that take the expand-sort-compress form: at most fmax products
 // (half the group's table), and at most 2 products per output (few repeated
 // columns; measured equal to 4 and better than 1.5 on the Galerkin rows).
-__device__ __forceinline__ bool esc_fits(const PhaseArgs &A, int64_t idx, int64_t fmax) {
-  const uint64_t e = A.list[idx];
-  const int64_t g = A.base[int(e >> 40)] + int64_t(e & ((uint64_t(1) << 40) - 1));
-  const int64_t f = A.rowf[g], c = A.rowc[g];
-  return f <= fmax && f <= 2 * c;
+__device__ __forceinline__ bool esc_fits(const RowMeta &m, int64_t fmax) {
+  return m.f <= fmax && m.f <= 2 * m.c;
 }
 
 // Group-level rows of class `cls`: the group leader fetches one row index at a
@@ -1176,15 +1287,19 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       const int64_t take = int64_t(v >> 48);
       if (i >= count) break;
       const int64_t e = min(count, i + take);
-      for (; i < e; ++i) {
+      // the chunk's metadata, one row per lane (take <= kChunk <= 32)
+      RowMeta mine{};
+      if (lane < e - i) mine = load_meta<NUM>(prods, A, base + i + lane);
+      for (int t = 0; i < e; ++i, ++t) {
         const long long t0 = clock64();
+        const RowMeta m = shfl_meta(mine, t);
         if constexpr (NUM) {
-          if (esc_fits(A, base + i, TMAXN / 2))
-            num_esc_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+          if (esc_fits(m, TMAXN / 2))
+            num_esc_row<G, TMAXN, PT, VT>(prods, A, m, slice, gm, gid, lane);
           else
-            num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+            num_hash_row<G, TMAXN, PT, VT>(prods, A, m, slice, gm, gid, lane);
         } else {
-          sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+          sym_hash_row<G, TMAXS, PT, VT>(prods, A, m, (int *)slice, gm, gid, lane);
         }
         prof_add(A, cls, t0, lane == 0);
       }
@@ -1203,13 +1318,14 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       const int64_t e = min(count, i + int64_t(v >> 48));
       for (; i < e; ++i) {
         const long long t0 = clock64();
+        const RowMeta m = load_meta<NUM>(prods, A, base + i);
         if constexpr (NUM) {
-          if (esc_fits(A, base + i, TMAXN / 2))
-            num_esc_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+          if (esc_fits(m, TMAXN / 2))
+            num_esc_row<G, TMAXN, PT, VT>(prods, A, m, slice, gm, gid, lane);
           else
-            num_hash_row<G, TMAXN, PT, VT>(prods, A, base + i, slice, gm, gid, lane);
+            num_hash_row<G, TMAXN, PT, VT>(prods, A, m, slice, gm, gid, lane);
         } else
-          sym_hash_row<G, TMAXS, PT, VT>(prods, A, base + i, (int *)slice, gm, gid, lane);
+          sym_hash_row<G, TMAXS, PT, VT>(prods, A, m, (int *)slice, gm, gid, lane);
         prof_add(A, cls, t0, lane == 0);
       }
     }
@@ -1278,9 +1394,11 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     } else {
       if constexpr (NUM)
-        num_hash_row<kThreads, kNumT1024, PT, VT>(prods, A, idx, smem, gm, 0, tid);
+        num_hash_row<kThreads, kNumT1024, PT, VT>(prods, A, load_meta<true>(prods, A, idx), smem,
+                                                  gm, 0, tid);
       else
-        sym_hash_row<kThreads, kSymT1024, PT, VT>(prods, A, idx, (int *)smem, gm, 0, tid);
+        sym_hash_row<kThreads, kSymT1024, PT, VT>(prods, A, load_meta<false>(prods, A, idx),
+                                                  (int *)smem, gm, 0, tid);
     }
     prof_add(A, c, t0, tid == 0);
     __syncthreads();
