@@ -180,6 +180,18 @@ int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out64);
 int tspg_spgemm_count(tspg_ctx *ctx, void *stream, const tspg_csr *A,
                       const tspg_csr *B, int64_t *mults, int64_t *c_nnz_upper);
 
+/* tspg_spgemm_count_mask — the flop-count pass fused with the stage mask of a
+ * SUMMA step on one GPU (the single-GPU form of SpaComm::spcomm_2D,
+ * include/spacomm.cuh:165-352): besides mults and c_nnz_upper it writes
+ * mask[ceil(ncols(A) / 8)] (device, LSB-first bytes) with bit k set exactly
+ * when column k of A holds an entry and row k of B is non-empty — the same
+ * bytes as SpaComm::intersect_bitmasks(gen_bitmask(colptr(A)),
+ * gen_bitmask(rowptr(B))) (spacomm.cuh:29-148), in one pass over A with no
+ * CSC copy of A.  Synchronises `stream`. */
+int tspg_spgemm_count_mask(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                           const tspg_csr *B, uint8_t *mask, int64_t *mults,
+                           int64_t *c_nnz_upper);
+
 /* tspg_spgemm — C = A·B, two-phase inside (symbolic, then numeric).
  * Replaces LocalMatrix::spgemm (include/KokkosWrap.hpp:367-391) and
  * cusparse_spgemm / _reuse / _mem (include/cusparse_helpers.cuh:908-1344).

@@ -56,3 +56,26 @@ def test_mod_pattern_filters(ctx):
             if i % ma == ka and i % mb == kb:
                 want[i // 8] |= 1 << (i % 8)
         np.testing.assert_array_equal(f, want)
+        fused, _, _ = ops.spgemm_count_mask(ctx, dA, dB)
+        np.testing.assert_array_equal(fused.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("bits", [(32, 32), (64, 32), (32, 64)])
+def test_count_mask_matches_separate_masks(ctx, bits):
+    # the fused flop count + stage mask against the oracle's gen / and of the
+    # column mask of A and the row mask of B, and against the plain count
+    from trident_b200 import ops
+    A = workloads.rmat(scale=11, edge_factor=8, seed=5)
+    tiles, _, _ = summa.cut_tiles(A, 4)
+    for i, s_, j in [(0, 1, 2), (3, 3, 0), (2, 0, 3), (1, 2, 1)]:
+        Ah, Bh = tiles[i][s_], tiles[s_][j]
+        dA, dB = Ah.to_device(rowptr_bits=bits[0]), Bh.to_device(rowptr_bits=bits[1])
+        mask, mults, upper = ops.spgemm_count_mask(ctx, dA, dB)
+        colptr = np.zeros(Ah.ncols + 1, np.int64)
+        np.add.at(colptr, Ah.col.astype(np.int64) + 1, 1)
+        want = oracle.bitmask_and(oracle.bitmask_gen(np.cumsum(colptr), Ah.ncols),
+                                  oracle.bitmask_gen(Bh.rowptr, Bh.nrows))
+        np.testing.assert_array_equal(mask.cpu().numpy(), want)
+        rm = oracle.row_mults(Ah, Bh)
+        assert mults == int(rm.sum()) and upper == int(np.minimum(rm, Bh.ncols).sum())
+        assert (mults, upper) == ops.spgemm_count(ctx, dA, dB)

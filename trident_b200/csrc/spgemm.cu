@@ -432,6 +432,93 @@ extern "C" int tspg_spgemm_count(tspg_ctx *ctx, void *stream,
   });
 }
 
+namespace tspg {
+
+// Flop count of A·B fused with the SUMMA stage mask: one warp per row of A;
+// entry (i, k) adds nnz(B row k) to the row's products and, when that row of B
+// is non-empty, sets bit k of the word mask.  Bit k ends up set exactly when
+// column k of A holds an entry and row k of B is non-empty, i.e. the AND of
+// the column mask of A and the row mask of B.
+template <typename APT, typename BPT>
+__global__ void k_count_mask(const APT *Ap, const int32_t *Aj, const BPT *Bp, int64_t m,
+                             int64_t n, uint32_t *mask, unsigned long long *tot) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long wm = 0, wu = 0;
+  for (int64_t r = warp; r < m; r += nwarps) {
+    const int64_t a0 = int64_t(Ap[r]), a1 = int64_t(Ap[r + 1]);
+    int64_t sum = 0;
+    for (int64_t q = a0 + lane; q < a1; q += 32) {
+      const int32_t k = __ldg(Aj + q);
+      const int64_t len = int64_t(Bp[k + 1]) - int64_t(Bp[k]);
+      sum += len;
+      if (len > 0) {
+        const uint32_t bit = 1u << (k & 31);
+        if (!(*(volatile uint32_t *)(mask + (k >> 5)) & bit)) atomicOr(mask + (k >> 5), bit);
+      }
+    }
+    sum = warp_sum(sum);
+    wm += (unsigned long long)sum;
+    wu += (unsigned long long)(sum < n ? sum : n);
+  }
+  if (lane == 0 && (wm | wu)) {
+    atomicAdd(tot, wm);
+    atomicAdd(tot + 1, wu);
+  }
+}
+
+// Word mask -> LSB-first byte mask: byte i holds bits k = 8i .. 8i + 7.
+__global__ void k_mask_bytes(const uint32_t *w, int64_t nbytes, uint8_t *out) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < nbytes) out[i] = uint8_t(w[i >> 2] >> ((i & 3) * 8));
+}
+
+template <typename APT, typename BPT>
+static void launch_count_mask(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A, const tspg_csr *B,
+                              uint32_t *words, unsigned long long *tot) {
+  k_count_mask<APT, BPT><<<grid_for(A->nrows * 32, 256, ctx->num_sms * 16), 256, 0, s>>>(
+      (const APT *)A->rowptr, A->col, (const BPT *)B->rowptr, A->nrows, B->ncols, words, tot);
+}
+
+}  // namespace tspg
+
+extern "C" int tspg_spgemm_count_mask(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                                      const tspg_csr *B, uint8_t *mask, int64_t *mults,
+                                      int64_t *c_nnz_upper) {
+  if (!ctx) return TSPG_EINVAL;
+  TSPG_TRY(check_pair(A, B));
+  const int64_t kdim = A->ncols, nbytes = (kdim + 7) / 8;
+  if (nbytes > 0 && !mask) return TSPG_EINVAL;
+  cudaStream_t s = (cudaStream_t)stream;
+  TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  Scratch sc(ctx, s);
+  uint32_t *words;
+  unsigned long long *tot;
+  TSPG_TRY(sc.get(&words, (kdim + 31) / 32));
+  TSPG_TRY(sc.get(&tot, 2));
+  TSPG_CUDA(ctx, cudaMemsetAsync(words, 0, sizeof(uint32_t) * ((kdim + 31) / 32 > 0 ? (kdim + 31) / 32 : 1), s));
+  TSPG_CUDA(ctx, cudaMemsetAsync(tot, 0, 2 * sizeof(unsigned long long), s));
+  if (A->nrows > 0) {
+    if (A->rowptr_bits == 32 && B->rowptr_bits == 32) launch_count_mask<int32_t, int32_t>(ctx, s, A, B, words, tot);
+    else if (A->rowptr_bits == 32) launch_count_mask<int32_t, int64_t>(ctx, s, A, B, words, tot);
+    else if (B->rowptr_bits == 32) launch_count_mask<int64_t, int32_t>(ctx, s, A, B, words, tot);
+    else launch_count_mask<int64_t, int64_t>(ctx, s, A, B, words, tot);
+    ctx->launches += 1;
+  }
+  if (nbytes > 0) {
+    k_mask_bytes<<<(unsigned)((nbytes + 255) / 256), 256, 0, s>>>(words, nbytes, mask);
+    ctx->launches += 1;
+  }
+  TSPG_CUDA(ctx, cudaGetLastError());
+  int64_t *h = ctx->h_words;
+  TSPG_CUDA(ctx, cudaMemcpyAsync(h, tot, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  TSPG_CUDA(ctx, cudaStreamSynchronize(s));
+  if (mults) *mults = h[0];
+  if (c_nnz_upper) *c_nnz_upper = h[1];
+  return TSPG_OK;
+}
+
 // C_out = C_in + A·B: the product goes to pool workspace, then the union merge
 // writes C_out (sp_mma_hybrid, include/cusparse_helpers.cuh:708-739, does the
 // same with KokkosKernels + csrgeam2).

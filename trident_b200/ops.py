@@ -166,6 +166,18 @@ def spgemm_count(ctx: Context, A: DeviceCSR, B: DeviceCSR, stream=None):
     return mults.value, up.value
 
 
+def spgemm_count_mask(ctx: Context, A: DeviceCSR, B: DeviceCSR, stream=None):
+    """(mask, mults, sum_i min(mults_i, ncols)): the flop-count pass fused
+    with the stage mask colmask(A) & rowmask(B) (ceil(ncols(A) / 8) bytes)."""
+    mults, up = C.c_int64(), C.c_int64()
+    a, b = A.abi(), B.abi()
+    n = (A.ncols + 7) // 8
+    out = torch.empty(max(n, 1), dtype=torch.uint8, device=A.rowptr.device)
+    check(lib.tspg_spgemm_count_mask(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b), out.data_ptr(),
+                                     C.byref(mults), C.byref(up)), "tspg_spgemm_count_mask")
+    return out[:n], mults.value, up.value
+
+
 def _finish(o: TspgCsrOut, rp, alloc: _TorchAlloc, val_bits: int) -> DeviceCSR:
     nnz = int(o.nnz)
     if nnz == 0:
@@ -273,7 +285,7 @@ def unpack(buf: torch.Tensor, nrows: int, ncols: int, nnz: int, major: int = TSP
     return DeviceCSR(nrows, ncols, rp, col, val, nnz=nnz)
 
 
-__all__ = ["Context", "Plan", "spgemm", "spgemm_count", "sp_mma", "spadd", "spgeam", "transpose",
+__all__ = ["Context", "Plan", "spgemm", "spgemm_count", "spgemm_count_mask", "sp_mma", "spadd", "spgeam", "transpose",
            "csc_to_csr", "gen_bitmask",
            "intersect_bitmasks", "compress", "unpack", "packed_bytes", "TSPG_ROWS", "TSPG_COLS",
            "TspgError", "TSPG_OK", "TSPG_ENOMEM"]

@@ -5,7 +5,8 @@ B(q,j), then sp_mma_hybrid) and the sparsity-aware exchange of
 include/spacomm.cuh:165-352 / 962-1091, with every "rank" of the q x q grid
 living on one GPU.  For stage q and output tile (i, j):
 
-  mask      = colmask(A_iq) & rowmask(B_qj)         (gen_bitmask + intersect)
+  mask      = colmask(A_iq) & rowmask(B_qj)         (fused into the flop-count
+                                                     pass: tspg_spgemm_count_mask)
   A'_iq     = csc_to_csr(unpack(pack_COLS(A_iq^CSC, mask)))
   B'_qj     = unpack(pack_ROWS(B_qj, mask))
   C_ij     += A'_iq · B'_qj                          (tspg_spgemm_acc)
@@ -62,19 +63,15 @@ class StageStats:
 def summa(ctx, A_tiles, B_tiles, q: int, use_masks: bool = True, stats: StageStats | None = None):
     """C tiles of A·B from device tiles A_tiles[i][k], B_tiles[k][j]."""
     C = [[None] * q for _ in range(q)]
-    # per-tile CSC of A (what the reference keeps with --Acsc) and the masks
+    # per-tile CSC of A (what the reference keeps with --Acsc), packed by columns
     A_csc = [[ops.transpose(ctx, A_tiles[i][k]) for k in range(q)] for i in range(q)]
-    a_cmask = [[ops.gen_bitmask(ctx, A_csc[i][k].rowptr, A_tiles[i][k].ncols) for k in range(q)]
-               for i in range(q)]
-    b_rmask = [[ops.gen_bitmask(ctx, B_tiles[k][j].rowptr, B_tiles[k][j].nrows) for j in range(q)]
-               for k in range(q)]
     for s in range(q):  # stage
         st = {"stage": s, "a_kept": 0, "b_kept": 0}
         for i in range(q):
             for j in range(q):
                 Aik, Bkj = A_tiles[i][s], B_tiles[s][j]
                 if use_masks:
-                    mask = ops.intersect_bitmasks(ctx, a_cmask[i][s], b_rmask[s][j])
+                    mask, _, _ = ops.spgemm_count_mask(ctx, Aik, Bkj)
                     Acsc = A_csc[i][s]  # nrows = tile cols: a CSR over the k dimension
                     abuf, akept = ops.compress(ctx, Acsc, mask, TSPG_ROWS)
                     Ap_csc = ops.unpack(abuf, Acsc.nrows, Acsc.ncols, akept, TSPG_ROWS,
