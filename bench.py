@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="rmat",
-                   choices=["rmat", "uniform", "batched", "rap", "served", "summa"])
+                   choices=["rmat", "uniform", "batched", "rap", "served", "summa", "coo"])
     p.add_argument("--rate", type=float, default=2000.0)
     p.add_argument("--duration", type=float, default=5.0)
     p.add_argument("--products", type=int, default=512)
@@ -697,6 +697,75 @@ def run_summa(args):
     return line
 
 
+def run_coo(args):
+    """COO -> CSR on the device (tspg_coo_to_csx) for the coordinates of R-MAT
+    scale --scale (default 20: 16.1M entries), shuffled by a seeded
+    permutation (the order a reader hands them over); the reference builds the
+    CSR on the host (std::sort of the triples by row, then an H2D copy).  One
+    step = one build from device-resident COO arrays into preallocated output
+    arrays; the CPU baseline is the oracle's restatement of the host builder
+    (numpy stable sort) on the same triples."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import oracle
+    from trident_b200 import ops, workloads
+    from trident_b200._lib import TSPG_ROWS, TspgCsrOut, check, lib
+    torch.cuda.set_device(0)
+    A = workloads.rmat(scale=args.scale, edge_factor=args.edge_factor, seed=args.seed)
+    rows = np.repeat(np.arange(A.nrows, dtype=np.int32), np.diff(A.rowptr))
+    perm = np.random.default_rng(args.seed).permutation(A.nnz)
+    hr, hc, hv = rows[perm], A.col[perm], A.val[perm]
+    dr, dc, dv = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (hr, hc, hv))
+    ctx = ops.Context(0)
+    M = ops.coo_to_csx(ctx, A.nrows, A.ncols, dr, dc, dv)
+    ok = bool(np.array_equal(M.col.cpu().numpy(), A.col) and np.array_equal(M.val.cpu().numpy(), A.val))
+    stream = torch.cuda.current_stream()
+
+    def step():
+        o = TspgCsrOut()
+        o.nrows, o.ncols = A.nrows, A.ncols
+        o.rowptr, o.rowptr_bits, o.val_bits = M.rowptr.data_ptr(), 64, 64
+        o.col, o.val, o.capacity = M.col.data_ptr(), M.val.data_ptr(), A.nnz
+        check(lib.tspg_coo_to_csx(ctx.h, stream.cuda_stream, A.nrows, A.ncols, A.nnz, dr.data_ptr(),
+                                  dc.data_ptr(), dv.data_ptr(), 64, TSPG_ROWS, C.byref(o)), "tspg_coo_to_csx")
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    clk = ClockSampler(0)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    algo = A.nnz * (4 + 4 + 8) + A.nnz * (4 + 8) + (A.nrows + 1) * 8  # COO read, CSR written
+    t0 = time.perf_counter()
+    oracle.coo_to_csx(A.nrows, hr, hc, hv)
+    cpu_s = time.perf_counter() - t0
+    line = {
+        "metric": "COO -> CSR build, M entries/s", "value": round(A.nnz / (ms * 1e-3) / 1e6, 1),
+        "unit": "M entries/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "dtype": "int32 indices, f64 values",
+        "data": "synthetic (seeded R-MAT coordinates, shuffled)",
+        "config": {"workload": f"rmat{args.scale}_coo", "rows": A.nrows, "nnz": A.nnz, "matches_generator": ok},
+        "roofline": {"bound": "hbm", "achieved": round(algo / (ms * 1e-3) / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4), "algorithmic_bytes": algo},
+        "cpu_baseline": {"value": round(A.nnz / cpu_s / 1e6, 1), "unit": "M entries/s", "cores": 1, "kind": "port",
+                         "sample": f"the whole workload, numpy stable sort by (row, col, position), {cpu_s:.1f} s"},
+        "clocks": clocks,
+    }
+    ctx.close()
+    return line
+
+
 def apply_tuning(ctx, name):
     """Apply the committed autotuner file of a workload (trident_b200/tuning/
     <name>.json, written by `python -m trident_b200.tune`), if there is one;
@@ -711,9 +780,9 @@ def apply_tuning(ctx, name):
 
 def main():
     args = parse()
-    if args.impl == "ours" and args.workload in ("batched", "rap", "served", "summa"):
+    if args.impl == "ours" and args.workload in ("batched", "rap", "served", "summa", "coo"):
         fn = {"batched": run_batched, "rap": run_rap, "served": run_served,
-              "summa": run_summa}[args.workload]
+              "summa": run_summa, "coo": run_coo}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
     rank = int(os.environ.get("RANK", 0))

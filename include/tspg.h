@@ -236,6 +236,22 @@ int tspg_spgemm_acc(tspg_ctx *ctx, void *stream, const tspg_csr *A,
 int tspg_transpose(tspg_ctx *ctx, void *stream, const tspg_csr *M,
                    tspg_csr_out *T);
 
+/* tspg_coo_to_csx — device COO (int32 row and column indices, values) to a
+ * compressed matrix: CSR for major = TSPG_ROWS (out: nrows x ncols), CSC for
+ * TSPG_COLS (out: the CSR of the transpose, ncols x nrows).  Replaces the host
+ * builders coo_to_row_csx / coo_to_col_csx(_contig) and coo_to_kokkos_crs /
+ * _ccs (include/cusparse_helpers.cuh:17-131, include/kokkos_helpers.cuh:52-352),
+ * which sort the triples on the host by the major index only and copy the
+ * result to the device.  Same pointer array and the same multiset of entries
+ * per segment, repeated entries kept; inside a segment entries come ordered
+ * by minor index, then input position (the reference leaves that order to
+ * std::sort).  Indices outside the shape: TSPG_EINVAL, nothing written.
+ * Output capacity / allocator as for SpGEMM.  Synchronises `stream`. */
+int tspg_coo_to_csx(tspg_ctx *ctx, void *stream, int64_t nrows, int64_t ncols,
+                    int64_t nnz, const int32_t *row, const int32_t *col,
+                    const void *val, int val_bits, int major,
+                    tspg_csr_out *out);
+
 /* ---- merge ------------------------------------------------------------------
  * tspg_spadd — C = A + B, union pattern, alpha = beta = 1.  Replaces
  * cusparse_spgeam (include/cusparse_helpers.cuh:799-905) and

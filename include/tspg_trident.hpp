@@ -284,6 +284,32 @@ struct LocalMatrix {
   Csx<IT, VT> get_csx() const { return storage.view(); }
 };
 
+// coo_to_row_csx / coo_to_col_csx (cusparse_helpers.cuh:17-131) and
+// coo_to_kokkos_crs / coo_to_kokkos_ccs (kokkos_helpers.cuh:52-352): triples
+// sorted by the major index and compressed — here on the device, from device
+// COO arrays, into a grow-only buffer (CSC comes out as the CSR of the
+// transpose: ptr over columns, row indices).  Repeated entries are kept.
+template <typename IT, typename VT>
+void coo_to_csx(Context &ctx, MajorDim major, IT nrows, IT ncols, IT nnz, const IT *d_row,
+                const IT *d_col, const VT *d_val, CsxBuffers<IT, VT> &out,
+                cudaStream_t s = nullptr) {
+  const bool rows = major == MajorDim::ROWS;
+  tspg_csr_out o = out.out(rows ? nrows : ncols, rows ? ncols : nrows);
+  TSPG_TRIDENT_CHECK(tspg_coo_to_csx(ctx.get(), s, nrows, ncols, nnz, d_row, d_col, d_val,
+                                     int(sizeof(VT) * 8), int(major), &o));
+  out.commit(o);
+}
+template <typename IT, typename VT>
+void coo_to_row_csx(Context &ctx, IT nrows, IT ncols, IT nnz, const IT *d_row, const IT *d_col,
+                    const VT *d_val, CsxBuffers<IT, VT> &out, cudaStream_t s = nullptr) {
+  coo_to_csx(ctx, MajorDim::ROWS, nrows, ncols, nnz, d_row, d_col, d_val, out, s);
+}
+template <typename IT, typename VT>
+void coo_to_col_csx(Context &ctx, IT nrows, IT ncols, IT nnz, const IT *d_row, const IT *d_col,
+                    const VT *d_val, CsxBuffers<IT, VT> &out, cudaStream_t s = nullptr) {
+  coo_to_csx(ctx, MajorDim::COLS, nrows, ncols, nnz, d_row, d_col, d_val, out, s);
+}
+
 // cusparse_spgeam (cusparse_helpers.cuh:799-905): C_accum = C_prod + C_local.
 template <typename IT, typename VT>
 void cusparse_spgeam(Context &ctx, const Csx<IT, VT> &C_prod, CsxBuffers<IT, VT> &C_local,

@@ -146,3 +146,21 @@ def pack(ptr, idx, val, mask):
     kept = lib.orc_pack(_p(p), length, _p(idx), _p(val), val.dtype.itemsize, _p(mask), _p(optr), _p(oidx),
                         _p(oval))
     return optr, oidx[:kept], oval[:kept]
+
+
+def coo_to_csx(nmaj: int, maj, mnr, val):
+    """COO -> compressed by `maj`: the host builders coo_to_row_csx /
+    coo_to_col_csx (include/cusparse_helpers.cuh:17-131) and coo_to_kokkos_crs
+    / _ccs (include/kokkos_helpers.cuh:52-352) sort the triples by the major
+    index (std::sort, so the order inside a segment is unspecified), count each
+    major index into ptr[i + 1], take the inclusive scan and emit the minor
+    indices and values in sorted order, repeated entries kept.  Restated with
+    the order inside a segment fixed to (minor index, input position), the
+    order the device builder produces.  Returns (ptr int64, minor int32, val)."""
+    maj = np.asarray(maj, dtype=np.int64)
+    mnr = np.asarray(mnr, dtype=np.int64)
+    order = np.lexsort((np.arange(maj.size), mnr, maj))
+    ptr = np.zeros(nmaj + 1, dtype=np.int64)
+    np.add.at(ptr, maj + 1, 1)
+    ptr = np.cumsum(ptr)
+    return ptr, mnr[order].astype(np.int32), np.asarray(val)[order]

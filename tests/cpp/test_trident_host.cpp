@@ -1,7 +1,8 @@
 // C++ host test of include/tspg_trident.hpp on a GPU: the known answers of the
 // reference's test/test_compression.cu (gen_bitmask :550-590, tmp_test1
-// :106-238 with the production MASK_SIZE = 8) and a two-stage sp_mma /
-// sp_mma_hybrid accumulation checked against a dense product.
+// :106-238 with the production MASK_SIZE = 8), a two-stage sp_mma /
+// sp_mma_hybrid accumulation checked against a dense product, csc_to_csr and
+// the COO builders.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -144,6 +145,33 @@ int main() {
     auto t = dense(T.get_csx());
     for (int i = 0; i < 3; ++i)
       for (int k = 0; k < 4; ++k) EXPECT(t[k * 3 + i] == a0[i * 4 + k], "csc_to_csr");
+    // COO -> CSR and CSC, with a repeated coordinate: both entries are kept
+    // and come in input order
+    {
+      std::vector<int32_t> r = {2, 0, 2, 1, 0, 2}, c = {1, 3, 0, 2, 3, 1};
+      std::vector<double> v = {1, 2, 3, 4, 5, 6};
+      int32_t *dr = to_dev(r), *dc = to_dev(c);
+      double *dv = to_dev(v);
+      CsxBuffers<int32_t, double> R, K;
+      coo_to_row_csx(ctx, 3, 4, 6, dr, dc, dv, R);
+      auto rp = to_host(R.d_node_rowptrs, 4);
+      auto ci = to_host(R.d_node_colinds, 6);
+      auto rv = to_host(R.d_node_vals, 6);
+      EXPECT(R.nnz == 6, "coo_to_row_csx nnz");
+      EXPECT((rp == std::vector<int32_t>{0, 2, 3, 6}), "coo_to_row_csx ptr");
+      EXPECT((ci == std::vector<int32_t>{3, 3, 2, 0, 1, 1}), "coo_to_row_csx idx");
+      EXPECT((rv == std::vector<double>{2, 5, 4, 3, 1, 6}), "coo_to_row_csx val");
+      coo_to_col_csx(ctx, 3, 4, 6, dr, dc, dv, K);
+      auto kp = to_host(K.d_node_rowptrs, 5);
+      auto ki = to_host(K.d_node_colinds, 6);
+      auto kv = to_host(K.d_node_vals, 6);
+      EXPECT((kp == std::vector<int32_t>{0, 1, 3, 4, 6}), "coo_to_col_csx ptr");
+      EXPECT((ki == std::vector<int32_t>{2, 2, 2, 1, 0, 0}), "coo_to_col_csx idx");
+      EXPECT((kv == std::vector<double>{3, 1, 6, 4, 2, 5}), "coo_to_col_csx val");
+      cudaFree(dr);
+      cudaFree(dc);
+      cudaFree(dv);
+    }
   }
   std::printf(failures ? "FAILED %d\n" : "ALL OK\n", failures);
   return failures ? 1 : 0;

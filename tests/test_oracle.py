@@ -137,3 +137,34 @@ def test_bmtx_values_vs_scipy():
     np.testing.assert_array_equal(S.indptr, rp)
     np.testing.assert_array_equal(S.indices, cj)
     np.testing.assert_allclose(S.data, cx, rtol=1e-13)
+
+
+def test_coo_to_csx_follows_reference_steps():
+    # the reference's host builder, step by step in plain Python: sort the
+    # triples by row, count rows into ptr[r + 1], inclusive scan, emit in
+    # sorted order; its order inside a row is unspecified (std::sort), so the
+    # rows are compared as multisets and the oracle's order checked separately
+    rng = np.random.default_rng(11)
+    n, m, nnz = 40, 30, 500
+    r = rng.integers(0, n, nnz)
+    c = rng.integers(0, m, nnz)
+    c[:50] = c[50:100]
+    r[:50] = r[50:100]  # repeated coordinates
+    v = rng.uniform(-1, 1, nnz)
+    trip = sorted(zip(r.tolist(), c.tolist(), v.tolist()), key=lambda t: t[0])
+    ptr = [0] * (n + 1)
+    for t in trip:
+        ptr[t[0] + 1] += 1
+    for i in range(n):
+        ptr[i + 1] += ptr[i]
+    optr, ocol, oval = oracle.coo_to_csx(n, r, c, v)
+    assert optr.tolist() == ptr
+    for i in range(n):
+        want = sorted((t[1], t[2]) for t in trip if t[0] == i)
+        got = sorted(zip(ocol[ptr[i]:ptr[i + 1]].tolist(), oval[ptr[i]:ptr[i + 1]].tolist()))
+        assert got == want
+        seg = ocol[ptr[i]:ptr[i + 1]]
+        assert np.all(np.diff(seg) >= 0)
+    # equal coordinates keep their input order
+    pos = np.lexsort((np.arange(nnz), c, r))
+    np.testing.assert_array_equal(oval, v[pos])

@@ -123,6 +123,7 @@ def _load() -> C.CDLL:
         "tspg_spgemm_acc": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(TspgCsr), P(TspgCsrOut), i32]),
         "tspg_spadd": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(TspgCsrOut)]),
         "tspg_transpose": (i32, [vp, vp, P(TspgCsr), P(TspgCsrOut)]),
+        "tspg_coo_to_csx": (i32, [vp, vp, i64, i64, i64, vp, vp, vp, i32, i32, P(TspgCsrOut)]),
         "tspg_bitmask_gen": (i32, [vp, vp, vp, i32, i64, vp]),
         "tspg_bitmask_and": (i32, [vp, vp, vp, vp, i64, vp]),
         "tspg_pack": (i32, [vp, vp, P(TspgCsr), i32, vp, vp, sz, vp, P(i64)]),

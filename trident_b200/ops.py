@@ -13,7 +13,7 @@ import ctypes as C
 
 import torch
 
-from ._lib import (ALLOC_FN, TSPG_COLS, TSPG_ENOMEM, TSPG_OK, TSPG_ROWS, TspgCsr, TspgTuning,
+from ._lib import (ALLOC_FN, TSPG_COLS, TSPG_EINVAL, TSPG_ENOMEM, TSPG_OK, TSPG_ROWS, TspgCsr, TspgTuning,
                    TspgCsrOut, TspgError, check, lib)
 from .csr import DeviceCSR
 
@@ -233,6 +233,25 @@ def transpose(ctx: Context, M: DeviceCSR, rowptr_bits: int = 64, stream=None) ->
 csc_to_csr = transpose
 
 
+def coo_to_csx(ctx: Context, nrows: int, ncols: int, row: torch.Tensor, col: torch.Tensor,
+               val: torch.Tensor, major: int = TSPG_ROWS, rowptr_bits: int = 64,
+               stream=None) -> DeviceCSR:
+    """Device COO (int32 row, col; FP64 / FP32 values) -> CSR (TSPG_ROWS) or
+    CSC (TSPG_COLS, returned as the CSR of the transpose); repeated entries
+    kept, each segment ordered by minor index then input position."""
+    nnz = int(row.numel())
+    if col.numel() != nnz or val.numel() != nnz or row.dtype != torch.int32 or col.dtype != torch.int32:
+        raise TspgError(TSPG_EINVAL, "coo_to_csx (int32 row / col and values of one length)")
+    vb = 64 if val.dtype == torch.float64 else 32
+    nmaj, nmin = (nrows, ncols) if major == TSPG_ROWS else (ncols, nrows)
+    rp = torch.empty(nmaj + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64, device=row.device)
+    alloc = _TorchAlloc(row.device)
+    o = _out_struct(nmaj, nmin, rp, vb, alloc=alloc)
+    check(lib.tspg_coo_to_csx(ctx.h, _stream_ptr(stream), nrows, ncols, nnz, row.data_ptr(), col.data_ptr(),
+                              val.data_ptr(), vb, major, C.byref(o)), "tspg_coo_to_csx")
+    return _finish(o, rp, alloc, vb)
+
+
 def gen_bitmask(ctx: Context, ptr: torch.Tensor, n: int, stream=None) -> torch.Tensor:
     """Bit i of the mask = segment i of ptr non-empty (SpaComm::gen_bitmask, MASK_SIZE 8)."""
     out = torch.empty(max((n + 7) // 8, 1), dtype=torch.uint8, device=ptr.device)
@@ -286,7 +305,7 @@ def unpack(buf: torch.Tensor, nrows: int, ncols: int, nnz: int, major: int = TSP
 
 
 __all__ = ["Context", "Plan", "spgemm", "spgemm_count", "spgemm_count_mask", "sp_mma", "spadd", "spgeam", "transpose",
-           "csc_to_csr", "gen_bitmask",
+           "csc_to_csr", "coo_to_csx", "gen_bitmask",
            "intersect_bitmasks", "compress", "unpack", "packed_bytes", "TSPG_ROWS", "TSPG_COLS",
            "TspgError", "TSPG_OK", "TSPG_ENOMEM"]
 
