@@ -318,6 +318,27 @@ size_t tspg_packed_bytes(int64_t nnz, int64_t ptr_len, int val_bits,
 int tspg_unpack(const void *buf, int64_t nrows, int64_t ncols, int major,
                 int64_t nnz, int val_bits, int ptr_bits, tspg_csr *out);
 
+/* ---- Markov clustering updates -----------------------------------------------------
+ * The per-iteration matrix updates of the reference's MCL driver
+ * (src/mcl.cu:56-149), which copies its tile to the host for each of them.
+ * Row sums are over the rows of M alone (the reference then adds the partial
+ * sums of a process row with MPI_Allreduce; on one GPU the tile holds whole
+ * rows).
+ * tspg_mcl_normalize: every row divided by its sum; a row whose sum is
+ *   <= 1e-20 becomes zeros (normalize, mcl.cu:97-127).
+ * tspg_mcl_inflate: every value raised to `power`, then normalized
+ *   (inflation, mcl.cu:130-149).
+ * Both write M's values (same pattern) to val_out, which may be M->val.
+ * tspg_mcl_prune: the entries with |v| > tol, in their order, as a new CSR
+ *   (prune, mcl.cu:56-93); output capacity / allocator as for SpGEMM;
+ *   synchronises `stream`. */
+int tspg_mcl_normalize(tspg_ctx *ctx, void *stream, const tspg_csr *M,
+                       void *val_out);
+int tspg_mcl_inflate(tspg_ctx *ctx, void *stream, const tspg_csr *M,
+                     double power, void *val_out);
+int tspg_mcl_prune(tspg_ctx *ctx, void *stream, const tspg_csr *M, double tol,
+                   tspg_csr_out *out);
+
 /* ---- batched products ----------------------------------------------------------
  * Many independent products C_i = A_i·B_i of uneven sizes in one persistent
  * launch per phase, fed by a device work queue; each phase is a CUDA graph

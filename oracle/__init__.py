@@ -164,3 +164,32 @@ def coo_to_csx(nmaj: int, maj, mnr, val):
     np.add.at(ptr, maj + 1, 1)
     ptr = np.cumsum(ptr)
     return ptr, mnr[order].astype(np.int32), np.asarray(val)[order]
+
+
+def mcl_normalize(rowptr, val):
+    """Rows scaled to sum 1; a row whose sum is <= 1e-20 becomes zeros
+    (normalize, src/mcl.cu:97-127: row sums in row order, then v / s)."""
+    rp = np.asarray(rowptr, dtype=np.int64)
+    v = np.array(val, copy=True)
+    for i in range(rp.size - 1):
+        seg = v[rp[i]:rp[i + 1]]
+        s = seg.sum(dtype=v.dtype)
+        v[rp[i]:rp[i + 1]] = seg / s if s > 1e-20 else 0
+    return v
+
+
+def mcl_inflate(rowptr, val, power):
+    """Values raised to `power`, then normalized (inflation, src/mcl.cu:130-149)."""
+    v = np.power(np.asarray(val), np.asarray(power, dtype=np.asarray(val).dtype))
+    return mcl_normalize(rowptr, v)
+
+
+def mcl_prune(rowptr, col, val, tol):
+    """The entries with |v| > tol in their order, with the new row offsets
+    (prune, src/mcl.cu:56-93: per-row kept counts, inclusive scan)."""
+    rp = np.asarray(rowptr, dtype=np.int64)
+    v = np.asarray(val)
+    keep = np.abs(v) > np.asarray(tol, dtype=v.dtype)
+    rows = np.repeat(np.arange(rp.size - 1), np.diff(rp))
+    cnt = np.bincount(rows[keep], minlength=rp.size - 1)
+    return np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64), np.asarray(col)[keep], v[keep]

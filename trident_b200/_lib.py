@@ -124,6 +124,9 @@ def _load() -> C.CDLL:
         "tspg_spadd": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(TspgCsrOut)]),
         "tspg_transpose": (i32, [vp, vp, P(TspgCsr), P(TspgCsrOut)]),
         "tspg_coo_to_csx": (i32, [vp, vp, i64, i64, i64, vp, vp, vp, i32, i32, P(TspgCsrOut)]),
+        "tspg_mcl_normalize": (i32, [vp, vp, P(TspgCsr), vp]),
+        "tspg_mcl_inflate": (i32, [vp, vp, P(TspgCsr), C.c_double, vp]),
+        "tspg_mcl_prune": (i32, [vp, vp, P(TspgCsr), C.c_double, P(TspgCsrOut)]),
         "tspg_bitmask_gen": (i32, [vp, vp, vp, i32, i64, vp]),
         "tspg_bitmask_and": (i32, [vp, vp, vp, vp, i64, vp]),
         "tspg_pack": (i32, [vp, vp, P(TspgCsr), i32, vp, vp, sz, vp, P(i64)]),

@@ -252,6 +252,34 @@ def coo_to_csx(ctx: Context, nrows: int, ncols: int, row: torch.Tensor, col: tor
     return _finish(o, rp, alloc, vb)
 
 
+def mcl_normalize(ctx: Context, M: DeviceCSR, stream=None) -> DeviceCSR:
+    """Rows of M scaled to sum 1 in place (rows summing to <= 1e-20 become 0)."""
+    m = M.abi()
+    check(lib.tspg_mcl_normalize(ctx.h, _stream_ptr(stream), C.byref(m), M.val.data_ptr()),
+          "tspg_mcl_normalize")
+    return M
+
+
+def mcl_inflate(ctx: Context, M: DeviceCSR, power: float = 2.0, stream=None) -> DeviceCSR:
+    """Values of M raised to `power`, then rows normalized, in place."""
+    m = M.abi()
+    check(lib.tspg_mcl_inflate(ctx.h, _stream_ptr(stream), C.byref(m), float(power), M.val.data_ptr()),
+          "tspg_mcl_inflate")
+    return M
+
+
+def mcl_prune(ctx: Context, M: DeviceCSR, tol: float, rowptr_bits: int = 64, stream=None) -> DeviceCSR:
+    """The entries of M with |v| > tol, as a new CSR."""
+    rp = torch.empty(M.nrows + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64,
+                     device=M.rowptr.device)
+    alloc = _TorchAlloc(M.rowptr.device)
+    o = _out_struct(M.nrows, M.ncols, rp, M.val_bits, alloc=alloc)
+    m = M.abi()
+    check(lib.tspg_mcl_prune(ctx.h, _stream_ptr(stream), C.byref(m), float(tol), C.byref(o)),
+          "tspg_mcl_prune")
+    return _finish(o, rp, alloc, M.val_bits)
+
+
 def gen_bitmask(ctx: Context, ptr: torch.Tensor, n: int, stream=None) -> torch.Tensor:
     """Bit i of the mask = segment i of ptr non-empty (SpaComm::gen_bitmask, MASK_SIZE 8)."""
     out = torch.empty(max((n + 7) // 8, 1), dtype=torch.uint8, device=ptr.device)
@@ -305,7 +333,7 @@ def unpack(buf: torch.Tensor, nrows: int, ncols: int, nnz: int, major: int = TSP
 
 
 __all__ = ["Context", "Plan", "spgemm", "spgemm_count", "spgemm_count_mask", "sp_mma", "spadd", "spgeam", "transpose",
-           "csc_to_csr", "coo_to_csx", "gen_bitmask",
+           "csc_to_csr", "coo_to_csx", "mcl_normalize", "mcl_inflate", "mcl_prune", "gen_bitmask",
            "intersect_bitmasks", "compress", "unpack", "packed_bytes", "TSPG_ROWS", "TSPG_COLS",
            "TspgError", "TSPG_OK", "TSPG_ENOMEM"]
 
