@@ -160,6 +160,22 @@ def cpu_baseline(A, mults_total, seconds):
 
 
 # ---------------------------------------------------------------- our arm
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """The job's step time: the slowest rank's (every rank calls this, in the
+    same order, after its own timed region)."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_gflops(mults: int, ms: float, world: int) -> float:
+    """Whole-job GFLOP/s of `world` replicas that each did 2 x mults in ms."""
+    return 2.0 * mults / (ms * 1e-3) / 1e9 * world
+
+
 def run_ours(args, rank, world):
     import ctypes as C
 
@@ -227,13 +243,8 @@ def run_ours(args, rank, world):
     check(lib.tspg_ctx_phase_timing(ctx.h, 0), "phase timing")
     launches1 = C.c_int64()
     lib.tspg_ctx_stats(ctx.h, C.byref(launches1))
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    flops = 2.0 * mults
-    value = flops / (ms * 1e-3) / 1e9 * world
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    value = replica_gflops(mults, ms, world)
 
     # roofline of the dominant persistent kernel
     bytes_a = csr_bytes(A.nrows, A.nnz, 4)
@@ -359,13 +370,9 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
     h2d = (hrp.numel() * 4 + hcol.numel() * 4 + hval.numel() * 8)
-    return {"value": round(2.0 * mults / (ms * 1e-3) / 1e9 * world, 3), "unit": "GFLOP/s",
+    return {"value": round(replica_gflops(mults, ms, world), 3), "unit": "GFLOP/s",
             "ms_per_step": round(ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(c_bytes),
             "c_to_host": "pinned result arrays" if full else "pinned 1 GiB staging ring (host RAM < 2x C)",
             "steps": steps}
