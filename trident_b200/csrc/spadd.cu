@@ -4,32 +4,90 @@
 // bufferSize + Nnz + compute, five stream syncs, the nnz through the host) and
 // LocalMatrix::spadd (include/KokkosWrap.hpp:394-439: KK spadd symbolic +
 // numeric).  Rows are sorted and duplicate-free, so every entry finds its
-// output slot independently: an A entry at row position i lands at
-// i + |{b in B row : b < a}|, a B entry that is not in A at
-// j + |{a in A row : a < b}|.  Rows with up to kMergeHeavy entries in A and B
-// together: one warp per row; lanes take entries and binary search the other
-// row (which sits in L1 after the first probes).  Longer rows (the hub rows of
+// output slot from its rank in the other row.  Rows with up to kMergeHeavy
+// entries in A and B together: one warp per row, merging 32-column chunks of
+// both rows in registers (merge_row_warp; per-entry binary searches of the
+// other row, as first built, took twice as long).  Longer rows (the hub rows of
 // partial C tiles reach 10^5 entries, and one warp per such row left the merge
-// waiting on a handful of warps) are listed and merged by a whole CTA along a
-// merge path: thread t takes steps [t, t+1) x (|A|+|B|) / threads of the
-// merged sequence (A before B on equal columns).
+// waiting on a handful of warps) are listed and merged by a whole CTA: its
+// warps take the ranges between merge-path cuts of the row.
 #include "internal.cuh"
 #include "spgemm_kernels.cuh"
 
 namespace tspg {
 
-template <typename IT>
-__device__ __forceinline__ int64_t lower_bound_row(const int32_t *col, int64_t lo,
-                                                   int64_t hi, int32_t x) {
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (__ldg(col + mid) < x) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
 constexpr int64_t kMergeHeavy = 4096;  // rows above this go to the CTA merge
 constexpr int kMergeThreads = 512;
+
+// Chunked warp merge of one light row.  Each iteration loads the next 32
+// columns of A and of B (coalesced).  Every entry up to lim, the smaller of
+// the two chunk maxima, is final this iteration (entries past a full chunk are
+// larger than its maximum); its output position is its index in its chunk
+// plus its rank in the other chunk (a 5-step search over the other chunk's
+// registers by shuffles) minus the columns of both rows below it.  A column in
+// both rows leaves once, from A, with the two values added.  At least 32
+// entries leave per iteration and no global load depends on another.
+// WRITE = false returns the size of the union only; WRITE = true writes no
+// position at or past cap (the row's size from the count pass), so rows that
+// break the sorted / duplicate-free contract cannot write outside their row.
+template <bool WRITE, typename VT>
+__device__ __forceinline__ int64_t merge_row_warp(const int32_t *__restrict__ Aj,
+                                                  const VT *__restrict__ Ax, int64_t a0,
+                                                  int64_t a1, const int32_t *__restrict__ Bj,
+                                                  const VT *__restrict__ Bx, int64_t b0,
+                                                  int64_t b1, int32_t *__restrict__ cj,
+                                                  VT *__restrict__ cx, int64_t cap, int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const unsigned below = (1u << lane) - 1u;
+  int64_t pa = a0, pb = b0, out = 0;
+  while (pa < a1 || pb < b1) {
+    const bool va = pa + lane < a1, vb = pb + lane < b1;
+    const int32_t ai = va ? __ldg(Aj + pa + lane) : INT32_MAX;  // no column is INT32_MAX
+    const int32_t bi = vb ? __ldg(Bj + pb + lane) : INT32_MAX;
+    VT av = VT(0), bv = VT(0);
+    if constexpr (WRITE) {
+      if (va) av = __ldg(Ax + pa + lane);
+      if (vb) bv = __ldg(Bx + pb + lane);
+    }
+    const int32_t lastA = __shfl_sync(FULL, ai, 31), lastB = __shfl_sync(FULL, bi, 31);
+    const int32_t lim = min(pa + 32 <= a1 ? lastA : INT32_MAX, pb + 32 <= b1 ? lastB : INT32_MAX);
+    int ra = 0, rb = 0;  // entries of the other chunk below this lane's entry
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+      if (__shfl_sync(FULL, bi, ra + st - 1) < ai) ra += st;
+      if (__shfl_sync(FULL, ai, rb + st - 1) < bi) rb += st;
+    }
+    if (ra == 31 && lastB < ai) ra = 32;
+    if (rb == 31 && lastA < bi) rb = 32;
+    const int32_t bat = __shfl_sync(FULL, bi, ra & 31), aat = __shfl_sync(FULL, ai, rb & 31);
+    const bool ca = va && ai <= lim, cb = vb && bi <= lim;
+    const bool dupa = ca && ra < 32 && bat == ai, dupb = cb && rb < 32 && aat == bi;
+    const unsigned dm = __ballot_sync(FULL, dupa);
+    const int na = __popc(__ballot_sync(FULL, ca)), nb = __popc(__ballot_sync(FULL, cb));
+    if constexpr (WRITE) {
+      const VT bvat = __shfl_sync(FULL, bv, ra & 31);
+      if (ca) {
+        const int64_t pos = out + lane + ra - __popc(dm & below);
+        if (pos < cap) {
+          cj[pos] = ai;
+          cx[pos] = dupa ? av + bvat : av;
+        }
+      }
+      if (cb && !dupb) {
+        const unsigned mk = rb >= 32 ? FULL : ((1u << rb) - 1u);
+        const int64_t pos = out + lane + rb - __popc(dm & mk);
+        if (pos < cap) {
+          cj[pos] = bi;
+          cx[pos] = bv;
+        }
+      }
+    }
+    out += na + nb - __popc(dm);
+    pa += na;
+    pb += nb;
+  }
+  return out;
+}
 
 template <typename PTA, typename PTB>
 __global__ void __launch_bounds__(256)
@@ -44,33 +102,18 @@ __global__ void __launch_bounds__(256)
       if (lane == 0) heavy[atomicAdd((unsigned long long *)nheavy, 1ull)] = r;
       continue;
     }
-    int dup = 0;
-    if (b1 > b0) {
-      for (int64_t p = a0 + lane; p < a1; p += 32) {
-        const int32_t x = __ldg(Aj + p);
-        const int64_t q = lower_bound_row<int>(Bj, b0, b1, x);
-        dup += (q < b1 && __ldg(Bj + q) == x);
-      }
-    }
-    dup = warp_sum(dup);
-    if (lane == 0) rowc[r] = int32_t((a1 - a0) + (b1 - b0) - dup);
+    const int64_t n = merge_row_warp<false, double>(Aj, nullptr, a0, a1, Bj, nullptr, b0, b1,
+                                                    nullptr, nullptr, 0, lane);
+    if (lane == 0) rowc[r] = int32_t(n);
   }
 }
 
-// Output rank of a column x of the union row: |{a < x}| + |{b < x}| minus
-// the columns below x present in both rows.  The fill walks A's row in warp
-// chunks, flags A entries that also occur in B (binary search), keeps the
-// running exclusive count of those flags in dpre[] (one int per A entry) and
-// writes every A entry; B entries absent from A then look their rank up
-// through dpre at their lower bound in A.
 template <typename PTA, typename PTB, typename VT>
 __global__ void __launch_bounds__(256)
     k_spadd_fill(int64_t m, const PTA *Ap, const int32_t *Aj, const VT *Ax,
                  const PTB *Bp, const int32_t *Bj, const VT *Bx,
-                 const int64_t *cp, void *Cp, int cp_bits, int32_t *Cj, VT *Cx,
-                 int32_t *dpre) {
+                 const int64_t *cp, void *Cp, int cp_bits, int32_t *Cj, VT *Cx) {
   const int lane = threadIdx.x & 31;
-  const unsigned below = (1u << lane) - 1u;
   const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
   for (int64_t r = warp; r < m; r += nwarps) {
@@ -85,118 +128,80 @@ __global__ void __launch_bounds__(256)
       }
     }
     if ((a1 - a0) + (b1 - b0) > kMergeHeavy) continue;  // merged by k_spadd_heavy
-    int running = 0;
-    for (int64_t base = a0; base < a1; base += 32) {
-      const int64_t p = base + lane;
-      bool dup = false;
-      int32_t x = 0;
-      int64_t q = b0;
-      if (p < a1) {
-        x = __ldg(Aj + p);
-        q = lower_bound_row<int>(Bj, b0, b1, x);
-        dup = q < b1 && __ldg(Bj + q) == x;
-      }
-      const unsigned bal = __ballot_sync(0xffffffffu, dup);
-      const int pre = running + __popc(bal & below);
-      if (p < a1) {
-        dpre[p] = pre;
-        VT v = __ldg(Ax + p);
-        if (dup) v += __ldg(Bx + q);
-        const int64_t pos = o + (p - a0) + (q - b0) - pre;
-        Cj[pos] = x;
-        Cx[pos] = v;
-      }
-      running += __popc(bal);
-    }
-    __syncwarp();
-    for (int64_t q = b0 + lane; q < b1; q += 32) {
-      const int32_t x = __ldg(Bj + q);
-      const int64_t p = lower_bound_row<int>(Aj, a0, a1, x);
-      if (p < a1 && __ldg(Aj + p) == x) continue;
-      const int common = p < a1 ? dpre[p] : running;
-      const int64_t pos = o + (q - b0) + (p - a0) - common;
-      Cj[pos] = x;
-      Cx[pos] = __ldg(Bx + q);
-    }
-    __syncwarp();
+    merge_row_warp<true, VT>(Aj, Ax, a0, a1, Bj, Bx, b0, b1, Cj + o, Cx + o, cp[r + 1] - o, lane);
   }
 }
 
-// Merge path of one heavy row inside a CTA.  Thread t covers the merged
-// steps [d0, d1); an A entry equal to the B entry at the B cursor takes that
-// B value too (it may lie past the thread's range), and a B entry equal to the
-// A entry before it is skipped, so a column present in both rows is emitted
-// once whichever thread holds either half.  WRITE = false counts the row's
-// union size; WRITE = true writes the row at (cj, cx).
-template <bool WRITE, typename VT>
-__device__ int64_t merge_row_cta(const int32_t *__restrict__ aj, const VT *__restrict__ ax,
-                                 int64_t la, const int32_t *__restrict__ bj,
-                                 const VT *__restrict__ bx, int64_t lb, int64_t *tmp,
-                                 int32_t *cj, VT *cx) {
-  const int tid = threadIdx.x;
-  const int64_t tot = la + lb;
-  const int64_t d0 = tot * tid / kMergeThreads, d1 = tot * (tid + 1) / kMergeThreads;
-  // largest i with A[i-1] <= B[d0-i]: the A entries among the first d0 steps
-  int64_t lo = d0 > lb ? d0 - lb : 0, hi = d0 < la ? d0 : la;
+// Heavy rows: one CTA of kMergeWarps warps per row.  The merged sequence is
+// cut at kMergeWarps + 1 diagonals (merge path: the A entries among the first
+// d merged entries, A before B on equal columns); a column present in both
+// rows whose A entry falls before a cut and B entry after it moves whole to
+// the earlier range, so every range merges on its own.  Each warp merges its
+// range with merge_row_warp.  The count pass keeps the cuts and the per-warp
+// counts (meta: kMergeWarps counts, then kMergeWarps + 1 pairs of cuts per
+// listed row) for the fill pass.
+constexpr int kMergeWarps = kMergeThreads / 32;
+constexpr int kHeavyMeta = kMergeWarps + 2 * (kMergeWarps + 1);
+
+__device__ __forceinline__ void merge_cut(const int32_t *__restrict__ aj, int64_t la,
+                                          const int32_t *__restrict__ bj, int64_t lb, int64_t d,
+                                          int64_t &i, int64_t &j) {
+  int64_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
   while (lo < hi) {
     const int64_t mid = (lo + hi + 1) >> 1;
-    if (__ldg(aj + mid - 1) <= __ldg(bj + d0 - mid)) lo = mid; else hi = mid - 1;
+    if (__ldg(aj + mid - 1) <= __ldg(bj + d - mid)) lo = mid; else hi = mid - 1;
   }
-  int64_t i = lo, j = d0 - lo;
-  auto step = [&](bool emit, int64_t pos) -> int {  // 1 if the step makes an output
-    const bool take_a = i < la && (j >= lb || __ldg(aj + i) <= __ldg(bj + j));
-    if (take_a) {
-      if (emit) {
-        const int32_t x = __ldg(aj + i);
-        VT v = __ldg(ax + i);
-        if (j < lb && __ldg(bj + j) == x) v += __ldg(bx + j);
-        cj[pos] = x;
-        cx[pos] = v;
-      }
-      ++i;
-      return 1;
-    }
-    const int32_t x = __ldg(bj + j);
-    const bool dup = i > 0 && __ldg(aj + i - 1) == x;
-    if (emit && !dup) {
-      cj[pos] = x;
-      cx[pos] = __ldg(bx + j);
-    }
-    ++j;
-    return dup ? 0 : 1;
-  };
-  const int64_t si = i, sj = j;
-  int64_t n = 0;
-  for (int64_t d = d0; d < d1; ++d) n += step(false, 0);
-  int64_t all;
-  const int64_t base = group_excl_scan<kMergeThreads, int64_t>(n, tmp, 0, &all);
-  if constexpr (WRITE) {
-    i = si;
-    j = sj;
-    int64_t pos = base;
-    for (int64_t d = d0; d < d1; ++d) pos += step(true, pos);
-  }
-  return all;
+  i = lo;
+  j = d - lo;
+  // the B entry that follows an equal A entry: the diagonal after d takes it
+  // first (A is strictly increasing), so the next cut's j stays >= this one
+  if (i > 0 && j < lb && __ldg(aj + i - 1) == __ldg(bj + j)) ++j;
 }
 
-// The listed heavy rows, one CTA each (persistent over the list).
 template <bool WRITE, typename PTA, typename PTB, typename VT>
 __global__ void __launch_bounds__(kMergeThreads)
     k_spadd_heavy(const int64_t *heavy, const int64_t *nheavy, const PTA *Ap,
                   const int32_t *Aj, const VT *Ax, const PTB *Bp, const int32_t *Bj,
-                  const VT *Bx, int32_t *rowc, const int64_t *cp, int32_t *Cj, VT *Cx) {
-  __shared__ int64_t tmp[kMergeThreads / 32 + 1];
+                  const VT *Bx, int32_t *rowc, const int64_t *cp, int64_t *meta, int32_t *Cj,
+                  VT *Cx) {
+  __shared__ int64_t cnt[kMergeWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t nh = *nheavy;
   for (int64_t h = blockIdx.x; h < nh; h += gridDim.x) {
     const int64_t r = heavy[h];
     const int64_t a0 = Ap[r], a1 = Ap[r + 1], b0 = Bp[r], b1 = Bp[r + 1];
-    if constexpr (WRITE) {
-      merge_row_cta<true, VT>(Aj + a0, Ax + a0, a1 - a0, Bj + b0, Bx + b0, b1 - b0, tmp,
-                              Cj + cp[r], Cx + cp[r]);
+    const int64_t la = a1 - a0, lb = b1 - b0;
+    int64_t *mt = meta + h * kHeavyMeta;
+    int64_t *cuts = mt + kMergeWarps;  // (i, j) per diagonal
+    if constexpr (!WRITE) {
+      if (threadIdx.x <= kMergeWarps) {
+        int64_t i, j;
+        merge_cut(Aj + a0, la, Bj + b0, lb, (la + lb) * threadIdx.x / kMergeWarps, i, j);
+        cuts[2 * threadIdx.x] = i;
+        cuts[2 * threadIdx.x + 1] = j;
+      }
+      __syncthreads();  // the cuts are read back through L1-bypassing loads below
+      const int64_t i0 = __ldcg(cuts + 2 * w), j0 = __ldcg(cuts + 2 * w + 1);
+      const int64_t i1 = __ldcg(cuts + 2 * w + 2), j1 = __ldcg(cuts + 2 * w + 3);
+      const int64_t n = merge_row_warp<false, VT>(Aj + a0, nullptr, i0, i1, Bj + b0, nullptr, j0,
+                                                  j1, nullptr, nullptr, 0, lane);
+      if (lane == 0) {
+        mt[w] = n;
+        cnt[w] = n;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int64_t t = 0;
+        for (int k = 0; k < kMergeWarps; ++k) t += cnt[k];
+        rowc[r] = int32_t(t);
+      }
     } else {
-      const int64_t n = merge_row_cta<false, VT>(Aj + a0, nullptr, a1 - a0, Bj + b0, nullptr,
-                                                 b1 - b0, tmp, nullptr, nullptr);
-      if (threadIdx.x == 0) rowc[r] = int32_t(n);
+      const int64_t i0 = cuts[2 * w], j0 = cuts[2 * w + 1];
+      const int64_t i1 = cuts[2 * w + 2], j1 = cuts[2 * w + 3];
+      int64_t off = cp[r];
+      for (int k = 0; k < w; ++k) off += mt[k];
+      merge_row_warp<true, VT>(Aj + a0, Ax + a0, i0, i1, Bj + b0, Bx + b0, j0, j1, Cj + off,
+                               Cx + off, mt[w], lane);
     }
     __syncthreads();
   }
@@ -207,18 +212,18 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                       const tspg_csr *B, tspg_csr_out *C) {
   const int64_t m = A->nrows;
   Scratch sc(ctx, s);
-  int32_t *rowc, *dpre;
-  int64_t *cp, *partial, *heavy;
+  int32_t *rowc;
+  int64_t *cp, *partial, *heavy, *meta;
   const int64_t nb = (m + kScanTile - 1) / kScanTile;
   Sched *dummy;
   TSPG_TRY(sc.get(&rowc, m));
-  TSPG_TRY(sc.get(&dpre, A->nnz));
   TSPG_TRY(sc.get(&cp, m + 1));
   TSPG_TRY(sc.get(&partial, nb + 1));
   TSPG_TRY(sc.get(&dummy, 1));
   // heavy[0] = count of listed rows, heavy[1..] = the rows
   const int64_t max_heavy = (A->nnz + B->nnz) / (kMergeHeavy + 1) + 1;
   TSPG_TRY(sc.get(&heavy, max_heavy + 1));
+  TSPG_TRY(sc.get(&meta, max_heavy * kHeavyMeta));
   TSPG_CUDA(ctx, cudaMemsetAsync(heavy, 0, sizeof(int64_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(cp, 0, sizeof(int64_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(dummy, 0, sizeof(Sched), s));
@@ -229,7 +234,7 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                                                  heavy + 1, heavy);
     k_spadd_heavy<false, PTA, PTB, VT><<<ctx->num_sms * 2, kMergeThreads, 0, s>>>(
         heavy + 1, heavy, (const PTA *)A->rowptr, A->col, (const VT *)A->val,
-        (const PTB *)B->rowptr, B->col, (const VT *)B->val, rowc, nullptr, nullptr, nullptr);
+        (const PTB *)B->rowptr, B->col, (const VT *)B->val, rowc, nullptr, meta, nullptr, nullptr);
     k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial);
     k_scan_partials<<<1, 1024, 0, s>>>(partial, nb);
     k_scan_final<<<(unsigned)nb, kScanThreads, 0, s>>>(rowc, m, partial, nb, cp, dummy, nullptr);
@@ -257,10 +262,10 @@ static int spadd_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   }
   k_spadd_fill<PTA, PTB, VT><<<grid, 256, 0, s>>>(
       m, (const PTA *)A->rowptr, A->col, (const VT *)A->val, (const PTB *)B->rowptr,
-      B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val, dpre);
+      B->col, (const VT *)B->val, cp, C->rowptr, C->rowptr_bits, C->col, (VT *)C->val);
   k_spadd_heavy<true, PTA, PTB, VT><<<ctx->num_sms * 2, kMergeThreads, 0, s>>>(
       heavy + 1, heavy, (const PTA *)A->rowptr, A->col, (const VT *)A->val,
-      (const PTB *)B->rowptr, B->col, (const VT *)B->val, nullptr, cp, C->col, (VT *)C->val);
+      (const PTB *)B->rowptr, B->col, (const VT *)B->val, nullptr, cp, meta, C->col, (VT *)C->val);
   ctx->launches += 2;
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
