@@ -146,7 +146,7 @@ int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
  * min(products, ncols)) and num_lim[] (numeric phase, on the row's nnz); rows
  * above the last bound are DENSE rows.  hash_load = hash-table slots per key
  * (2, 4 or 8).  Bounds must be positive, non-decreasing and at most the table
- * capacities sym <= {512, 2048, 4096, 24576}, num <= {512, 1024, 2048, 8192}
+ * capacities sym <= {512, 2048, 4096, 24576}, num <= {256, 1024, 2048, 8192}
  * (the defaults); otherwise TSPG_EINVAL.  Applies to calls made after it;
  * results do not depend on it. */
 typedef struct tspg_tuning {

@@ -221,6 +221,10 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_phase<PT, VT, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
+  TSPG_CUDA(ctx, cudaFuncSetAttribute(k_groups<PT, VT, false>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupDynSmem));
+  TSPG_CUDA(ctx, cudaFuncSetAttribute(k_groups<PT, VT, true>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupDynSmem));
   // the graphs hold the row binning of their capture: a new tuning re-captures
   const bool retune = std::memcmp(&b->tune, &ctx->tune, sizeof(Tune)) != 0;
   const bool rebuild = b->dirty || !b->g1 || b->gstream != s || retune;
@@ -339,6 +343,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                    ctx->d_prof};
       phase_mark(ctx, 0, 0, s);
       k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+      k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 0, 1, s);
       k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(b->rowc, R, b->partial);
       k_scan_partials<<<1, 1024, 0, s>>>(b->partial, nb);
@@ -346,7 +351,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                                          b->sched + 1, b->rowf);
     }
     k_gather_offsets<<<(nprod + 256) / 256, 256, 0, s>>>(b->cp, b->d_base, nprod, b->offs);
-    b->g1_kernels = 2 + (!(flags & TSPG_F_B_SORTED) && b->RB > 0) + (R > 0 ? 7 : 0);
+    b->g1_kernels = 2 + (!(flags & TSPG_F_B_SORTED) && b->RB > 0) + (R > 0 ? 8 : 0);
     cudaMemcpyAsync(b->h_offs, b->offs, sizeof(int64_t) * (nprod + 1), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(b->h_offs + nprod + 1, &b->sched[0].max_a_row, sizeof(int64_t),
                     cudaMemcpyDeviceToHost, s);
@@ -410,10 +415,11 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                    b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
       phase_mark(ctx, 1, 0, s);
       k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+      k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 1, 1, s);
     }
     k_zero_rowptr<PT, VT><<<(nprod + 31) / 32, 32, 0, s>>>(prods, nprod);
-    b->g2_kernels = 2 + (R > 0 ? 3 : 0);
+    b->g2_kernels = 2 + (R > 0 ? 4 : 0);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (e != cudaSuccess) {
       ctx->last_cuda = (int)e;

@@ -17,7 +17,7 @@ namespace tspg {
 // tables hold key + FP64 value (192 KiB per CTA); a table has T = pow2 >=
 // load x the bound slots.
 constexpr int64_t kSymLim32 = 512, kSymLim128 = 2048, kSymLim256 = 4096, kSymLim1024 = 24576;
-constexpr int64_t kNumLim32 = 512, kNumLim128 = 1024, kNumLim256 = 2048, kNumLim1024 = 8192;
+constexpr int64_t kNumLim32 = 256, kNumLim128 = 1024, kNumLim256 = 2048, kNumLim1024 = 8192;
 
 // Runtime row-binning parameters (the autotuned part of the SpGEMM): upper
 // bounds of the warp / 128 / 256 / CTA group classes, symbolic on

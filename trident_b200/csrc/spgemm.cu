@@ -25,7 +25,14 @@ static int set_smem_attr() {
     cudaError_t e2 = cudaFuncSetAttribute(k_phase<PT, VT, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kDynSmem);
-    if (e1 != cudaSuccess || e2 != cudaSuccess) return TSPG_ECUDA;
+    cudaError_t e3 = cudaFuncSetAttribute(k_groups<PT, VT, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kGroupDynSmem);
+    cudaError_t e4 = cudaFuncSetAttribute(k_groups<PT, VT, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kGroupDynSmem);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
+      return TSPG_ECUDA;
     done = true;
   }
   return TSPG_OK;
@@ -143,6 +150,7 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                  nullptr, 0, ctx->d_words + kErrWord, ctx->d_prof};
     phase_mark(ctx, 0, 0, s);
     k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+    k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
     phase_mark(ctx, 0, 1, s);
     k_scan_reduce<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial);
     k_scan_partials<<<1, 1024, 0, s>>>(P->partial, P->nb);
@@ -150,7 +158,7 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                                                           P->nb, P->cp, P->sched + 1, P->rowf);
   }
   TSPG_CUDA(ctx, cudaGetLastError());
-  ctx->launches += 2 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 7 : 0);
+  ctx->launches += 2 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 8 : 0);
   int64_t *h = ctx->h_words;
   TSPG_CUDA(ctx, cudaMemcpyAsync(h, P->cp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   TSPG_CUDA(ctx, cudaMemcpyAsync(h + 1, &P->sched[0].total, 4 * sizeof(int64_t),
@@ -193,8 +201,9 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
                ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
   phase_mark(ctx, 1, 0, s);
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+  k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
   phase_mark(ctx, 1, 1, s);
-  ctx->launches += 4;
+  ctx->launches += 5;
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
 }

@@ -35,6 +35,13 @@ constexpr int kThreads = 512;   // persistent CTA: 16 warps x 128 registers
 constexpr int kTableSmem = 196608;              // hash tables / dense window
 constexpr int kCountSmem = 16384;               // radix-sort digit counters
 constexpr int kDynSmem = kTableSmem + kCountSmem;  // one CTA per SM
+// The group-row kernel (k_groups): 24 warps x 80 registers over the same
+// table space, so more rows are in flight per SM than the 16 warps of the
+// persistent CTA-row kernel (group rows are latency-bound: shared-memory
+// probes and the loads of short B rows); 1 KiB of digit counters per warp.
+constexpr int kGroupThreads = 768;
+constexpr int kGroupCountSmem = (kGroupThreads / 32) * 1024;
+constexpr int kGroupDynSmem = kTableSmem + kGroupCountSmem;
 
 // Row classes, heaviest first.  The first four are worked by the whole CTA
 // (items fetched by one thread); G256 / G128 / G32 rows are fetched by each
@@ -54,7 +61,7 @@ __host__ __device__ constexpr bool cls_dense(int c) { return c <= CLS_DENSE2; }
 
 constexpr int kSymT32 = 1024, kSymT128 = 4096, kSymT256 = 8192,
               kSymT1024 = 32768;
-constexpr int kNumT32 = 1024, kNumT128 = 2048, kNumT256 = 4096,
+constexpr int kNumT32 = 512, kNumT128 = 2048, kNumT256 = 4096,
               kNumT1024 = 16384;
 constexpr int kDenseW = 16384;           // numeric dense window (columns)
 constexpr int kDenseCurSmem = 8192;      // cursors kept in shared memory

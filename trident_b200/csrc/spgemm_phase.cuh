@@ -1244,7 +1244,9 @@ __device__ __forceinline__ bool esc_fits(const RowMeta &m, int64_t fmax) {
 template <int G, bool NUM, typename PT, typename VT>
 __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                            int cls, unsigned char *smem, PhaseShared &sh) {
-  constexpr int SLICE = NUM ? kTableSmem / (kThreads / G) : (kTableSmem * 2 / 3) / (kThreads / G);
+  constexpr int NG = kGroupThreads / G;  // groups of this size per CTA
+  // slices start on 16-byte boundaries (the tables are cleared with 16-byte stores)
+  constexpr int SLICE = (NUM ? kTableSmem / NG : (kTableSmem * 2 / 3) / NG) & ~15;
   constexpr int TMAXS = G == 256 ? kSymT256 : G == 128 ? kSymT128 : kSymT32;
   constexpr int TMAXN = G == 256 ? kNumT256 : G == 128 ? kNumT128 : kNumT32;
   static_assert(!NUM || TMAXN * 12 <= SLICE, "numeric slice");
@@ -1256,7 +1258,7 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   // digit counters nest like the slices: 1 KiB per warp, a group's counters
   // start at its first warp's (a warp's radix needs 32 digits x 16 items x 2 B)
   static_assert(32 * (TMAXN / (2 * G)) * (G / 32) * 2 <= (G / 32) * 1024, "counters");
-  static_assert((kThreads / 32) * 1024 <= kCountSmem, "counter space");
+  static_assert((kGroupThreads / 32) * 1024 <= kGroupCountSmem, "counter space");
   gm.cnt = (uint16_t *)(smem + kTableSmem + gid * (G / 32) * 1024);
   gm.tmp = sh.scan + slot * 33;
   gm.itmp = sh.itmp + slot * 18;
@@ -1270,7 +1272,7 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   // rows are taken in chunks (one counter atomic per chunk); the chunk shrinks
   // to one row as the class runs out so the tail stays balanced
   constexpr int64_t kChunk = G == 32 ? 16 : G == 128 ? 4 : 2;
-  const int64_t groups = int64_t(gridDim.x) * (kThreads / G);
+  const int64_t groups = int64_t(gridDim.x) * NG;
   while (true) {
     int64_t i;
     if constexpr (G == 32) {
@@ -1403,7 +1405,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     prof_add(A, c, t0, tid == 0);
     __syncthreads();
   }
-  // stage 2: nested groups, no CTA-wide barrier from here on
+}
+
+// The group classes (G256, G128, G32 rows), persistent: the CTA splits into
+// 256-thread groups, then 128-thread groups, then warps; each fetches its
+// rows on its own, and no CTA-wide barrier follows the set-up.
+template <typename PT, typename VT, bool NUM>
+__global__ void __launch_bounds__(kGroupThreads, 1)
+    k_groups(const ProdDev<PT, VT> *prods, PhaseArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ PhaseShared sh;
+  if (threadIdx.x < NCLS) {
+    sh.off[threadIdx.x] = A.S->off[threadIdx.x];
+    sh.cnt[threadIdx.x] = A.S->cnt[threadIdx.x];
+  }
+  __syncthreads();
   group_rows<256, NUM, PT, VT>(prods, A, CLS_G256, smem, sh);
   group_rows<128, NUM, PT, VT>(prods, A, CLS_G128, smem, sh);
   group_rows<32, NUM, PT, VT>(prods, A, CLS_G32, smem, sh);

@@ -28,9 +28,9 @@ import time
 # Candidate bounds per slot; each slot is capped by the table capacity of its
 # class (the defaults), and bounds stay non-decreasing over the classes.
 SYM_CAP = [512, 2048, 4096, 24576]
-NUM_CAP = [512, 1024, 2048, 8192]
+NUM_CAP = [256, 1024, 2048, 8192]
 SYM_CHOICES = [[128, 256, 512], [1024, 2048], [2048, 3072, 4096], [8192, 12288, 24576]]
-NUM_CHOICES = [[128, 256, 384, 512], [512, 768, 1024], [1024, 1536, 2048], [4096, 6144, 8192]]
+NUM_CHOICES = [[128, 192, 256], [512, 768, 1024], [1024, 1536, 2048], [4096, 6144, 8192]]
 LOAD_CHOICES = [2, 4]
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
