@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--workload", default="rmat",
                    choices=["rmat", "uniform", "batched", "rap", "served", "summa", "coo"])
     p.add_argument("--rate", type=float, default=2000.0)
+    p.add_argument("--lanes", type=int, default=3, help="server worker lanes (served)")
+    p.add_argument("--max-batch", type=int, default=64, help="requests per server batch (served)")
     p.add_argument("--duration", type=float, default=5.0)
     p.add_argument("--products", type=int, default=512)
     p.add_argument("--scale", type=int, default=20)
@@ -591,7 +593,7 @@ def run_served(args):
     kinds = rng.random(n_req) < 0.7
     picks = [int(rng.integers(0, len(ab_pool) if k else len(rap_pool))) for k in kinds]
     gaps = rng.exponential(1.0 / args.rate, size=n_req)
-    srv = ops.Server(ctx, mem_budget=120 << 30, lanes=3, max_batch=64)
+    srv = ops.Server(ctx, mem_budget=120 << 30, lanes=args.lanes, max_batch=args.max_batch)
     # warm-up: one request of each kind
     for t in (srv.submit(*ab_pool[0]), srv.submit(rap_pool[0][1], rap_pool[0][2], rap_pool[0][0])):
         srv.wait(t)
@@ -647,7 +649,7 @@ def run_served(args):
         "unit": "req/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic (resident pool: 24 A·B pairs, 8 R·A·P sets)",
         "config": {"tuning": tuning, "workload": "served", "rate": args.rate, "duration_s": args.duration, "requests": n_req,
-                   "ab_share": 0.7, "budget_gb": 120, "lanes": 3, "max_batch": 64},
+                   "ab_share": 0.7, "budget_gb": 120, "lanes": args.lanes, "max_batch": args.max_batch},
         "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
         "batches": stats["batches"], "loop_of_plain_calls": {"req_per_s": round(n_req / loop_s, 1)},
         "speedup_vs_loop": round(served / (n_req / loop_s), 3),

@@ -369,13 +369,13 @@ int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out);
 /* ---- serving ---------------------------------------------------------------------
  * A continuous-batching server for C = A·B and Galerkin C = R·(A·P) requests
  * with device-resident operands (borrowed until the request completes).
- * Requests wait in a FIFO; each of `lanes` worker threads (own context and
- * stream) takes the waiting requests (up to max_batch) whenever it frees up,
- * bounds their outputs with one batched flop-count pass, admits the FIFO
- * prefix that fits `mem_budget` bytes (the rest go back to the head of the
- * queue) and runs it as one batched product per stage, so batches formed
- * while others run overlap on the device.  Submission does no device work.
- * Results (int64 row offsets) stay valid until release. */
+ * Submission does no device work.  A bounding thread bounds the outputs of
+ * the submitted requests, in order, with batched flop-count passes; each of
+ * `lanes` worker threads (own context and stream) then admits from the head
+ * of that FIFO, in submission order, the requests (up to max_batch) that fit
+ * `mem_budget` bytes and runs them as one batched product per stage, so
+ * batches formed while others run overlap on the device.  Results (int64 row
+ * offsets) stay valid until release. */
 enum { TSPG_REQ_AB = 0, TSPG_REQ_RAP = 1 };
 typedef struct tspg_server tspg_server;
 typedef struct tspg_server_config {
@@ -387,6 +387,8 @@ typedef struct tspg_server_config {
  * which take ctx's row binning (tspg_ctx_set_tuning) at creation. */
 int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
                        tspg_server **out);
+/* Finishes the batches on the device, drops requests still waiting for
+ * admission and frees every result not yet released. */
 int tspg_server_destroy(tspg_server *s);
 /* kind TSPG_REQ_AB: C = A·B (R unused); TSPG_REQ_RAP: C = R·(A·B) with B the
  * prolongator.  Checks the shapes and enqueues; a request whose output bound

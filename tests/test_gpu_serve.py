@@ -93,3 +93,25 @@ def test_server_refuses_bad_shapes(ctx):
     assert e.value.status == TSPG_EINVAL
     assert srv.stats()["queued"] == 0
     srv.close()
+
+
+def test_server_admits_in_submission_order_under_a_tight_budget(ctx):
+    # a budget that holds a few requests at a time, three lanes claiming
+    # large batches, and a consumer that waits and releases in ticket order:
+    # a later request admitted before an earlier one would hold the budget
+    # the earlier one needs (the wait times out instead of hanging)
+    ops_pairs = [(workloads.poisson_rows(6000, 12.0, s), workloads.poisson_rows(6000, 12.0, s + 1))
+                 for s in (11, 13, 15, 17)]
+    dev = [(A.to_device(), B.to_device()) for A, B in ops_pairs]
+    mults, upper = ops.spgemm_count(ctx, *dev[0])
+    one = upper * 12 + 6001 * 8
+    srv = ops.Server(ctx, mem_budget=int(3.5 * one), lanes=3, max_batch=16)
+    want = [ops.spgemm(ctx, A, B).to_host() for A, B in dev]
+    tickets = [(k % 4, srv.submit(*dev[k % 4])) for k in range(48)]
+    for k, t in tickets:
+        res, _ = srv.wait(t, timeout_ms=60000)
+        _same(res.to_host(), want[k])
+        srv.release(t)
+    st = srv.stats()
+    assert st["completed"] == 48 and st["reserved"] == 0 and st["status"] == 0
+    srv.close()

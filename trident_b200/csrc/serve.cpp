@@ -1,12 +1,13 @@
 // serve.cpp — continuous-batching server for A·B and Galerkin R·A·P requests.
 //
 // Requests arrive on any host thread (tspg_server_submit) with device-resident
-// operands and wait in a FIFO; submission does no device work.  `lanes` worker
-// threads, each with its own context, stream and tspg_batch objects, take the
-// waiting requests (up to max_batch) when the lane frees up, bound every
-// output with one batched flop-count pass (sum_i min(mults_i, ncols), 12 bytes
-// per entry plus row offsets), admit the FIFO prefix that fits the device-
-// memory budget and put the rest back at the head of the queue.  The admitted
+// operands; submission does no device work.  A bounding thread (own context
+// and stream) takes them in order and bounds their outputs with one batched
+// flop-count pass per run of requests (sum_i min(mults_i, ncols), 12 bytes
+// per entry plus row offsets) into the admission queue.  `lanes` worker
+// threads, each with its own context, stream and tspg_batch objects, admit
+// from the head of that queue, under the server lock and in submission order,
+// the requests (up to max_batch) that fit the device-memory budget.  The admitted
 // requests run as one batched product per stage: stage 1 = all A·B requests
 // plus the A·P half of the R·A·P requests, stage 2 = R·(AP) for the R·A·P
 // requests.  Lanes run concurrently on their own streams, so a batch that
@@ -70,13 +71,16 @@ struct tspg_server {
   int device = 0;
   tspg_server_config cfg{};
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
-  std::deque<Req *> queue;
+  std::condition_variable cv_fresh, cv_work, cv_done;
+  std::deque<Req *> fresh;  // submitted, output not bounded yet
+  std::deque<Req *> queue;  // bounded, waiting for admission (submission order)
   std::unordered_map<int64_t, Req *> reqs;
   size_t reserved = 0;
   bool stop = false;
   int64_t next_ticket = 1;
   std::vector<std::thread> threads;
+  tspg_ctx *bctx = nullptr;  // context and stream of the bounding thread
+  cudaStream_t bstream = nullptr;
   std::vector<tspg_ctx *> lane_ctx;
   std::vector<cudaStream_t> lane_stream;
   int64_t batches = 0, completed = 0, rejected = 0;
@@ -156,70 +160,86 @@ int bound_requests(tspg_batch *bc, cudaStream_t s, const std::vector<Req *> &can
   return TSPG_OK;
 }
 
-void lane_main(tspg_server *S, int lane) {
+// The bounding thread: takes the submitted requests in order (a run of one
+// value width at a time), bounds their outputs with one batched count pass,
+// and appends them to the admission queue (or completes them with
+// TSPG_ENOMEM when the bound alone exceeds the budget).  Bounding ahead of
+// the lanes keeps the count passes, which wait for SMs behind the lanes'
+// persistent kernels, off the admission path.
+void bound_main(tspg_server *S) {
   cudaSetDevice(S->device);
-  tspg_ctx *ctx = S->lane_ctx[lane];
-  cudaStream_t s = S->lane_stream[lane];
-  tspg_batch *b1 = nullptr, *b2 = nullptr, *bc = nullptr;
-  tspg_batch_create(ctx, &b1);
-  tspg_batch_create(ctx, &b2);
-  tspg_batch_create(ctx, &bc);
-  std::vector<Req *> cand, take, back;
+  tspg_batch *bc = nullptr;
+  tspg_batch_create(S->bctx, &bc);
+  std::vector<Req *> cand;
   while (true) {
     cand.clear();
-    take.clear();
-    back.clear();
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
-      if (S->stop && S->queue.empty()) break;
-      // claim the head of the queue (one value width per batch)
-      while (!S->queue.empty() && (int)cand.size() < S->cfg.max_batch &&
-             (cand.empty() || S->queue.front()->A.val_bits == cand[0]->A.val_bits)) {
-        cand.push_back(S->queue.front());
-        S->queue.pop_front();
+      S->cv_fresh.wait(lk, [&] { return S->stop || !S->fresh.empty(); });
+      if (S->stop) break;
+      while (!S->fresh.empty() && cand.size() < 4096 &&
+             (cand.empty() || S->fresh.front()->A.val_bits == cand[0]->A.val_bits)) {
+        cand.push_back(S->fresh.front());
+        S->fresh.pop_front();
       }
     }
-    const int bst = bound_requests(bc, s, cand);
+    const int bst = bound_requests(bc, S->bstream, cand);
     bool rejected = false;
     {
-      std::unique_lock<std::mutex> lk(S->mu);
-      // FIFO admission by the memory budget; the head request is admitted
-      // whenever nothing else is reserved, unless it exceeds the budget alone
+      std::lock_guard<std::mutex> lk(S->mu);
       for (Req *r : cand) {
-        const bool fail = bst != TSPG_OK || r->reserve > S->cfg.mem_budget;
-        if (fail) {
+        if (bst != TSPG_OK || r->reserve > S->cfg.mem_budget) {
           r->status = bst != TSPG_OK ? bst : TSPG_ENOMEM;
           r->t_done = now_ms();
           r->done = true;
           S->rejected += 1;
           rejected = true;
-          continue;
-        }
-        if (back.empty() && (S->reserved + r->reserve <= S->cfg.mem_budget ||
-                             (S->reserved == 0 && take.empty()))) {
-          S->reserved += r->reserve;
-          r->admitted = true;
-          take.push_back(r);
         } else {
-          back.push_back(r);
+          S->queue.push_back(r);
         }
       }
-      for (auto it = back.rbegin(); it != back.rend(); ++it) S->queue.push_front(*it);
       if (bst != TSPG_OK) S->lane_error = bst;
+    }
+    S->cv_work.notify_all();
+    if (rejected) S->cv_done.notify_all();
+  }
+  tspg_batch_destroy(bc);
+}
+
+void lane_main(tspg_server *S, int lane) {
+  cudaSetDevice(S->device);
+  tspg_ctx *ctx = S->lane_ctx[lane];
+  cudaStream_t s = S->lane_stream[lane];
+  tspg_batch *b1 = nullptr, *b2 = nullptr;
+  tspg_batch_create(ctx, &b1);
+  tspg_batch_create(ctx, &b2);
+  std::vector<Req *> take;
+  while (true) {
+    take.clear();
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      if (S->stop) break;  // requests still waiting for admission are dropped
+      // FIFO admission by the memory budget, under the lock (no device work
+      // here), so requests are admitted in submission order across lanes; the
+      // head request is admitted whenever nothing else is reserved (its bound
+      // fits the budget alone); one value width per batch
+      while (!S->queue.empty() && (int)take.size() < S->cfg.max_batch) {
+        Req *r = S->queue.front();
+        if (!take.empty() && r->A.val_bits != take[0]->A.val_bits) break;
+        if (S->reserved + r->reserve > S->cfg.mem_budget && !(S->reserved == 0 && take.empty()))
+          break;
+        S->queue.pop_front();
+        S->reserved += r->reserve;
+        r->admitted = true;
+        take.push_back(r);
+      }
       if (take.empty()) {
-        if (rejected) {
-          lk.unlock();
-          S->cv_done.notify_all();
-          continue;
-        }
-        // budget held by other lanes: wait for a release
+        // budget held by admitted requests: wait for a release
         S->cv_done.wait_for(lk, std::chrono::milliseconds(1));
         continue;
       }
     }
-    if (rejected) S->cv_done.notify_all();
-    if (!back.empty()) S->cv_work.notify_one();
     const double t0 = now_ms();
     for (Req *r : take) r->t_start = t0;
     int st = TSPG_OK;
@@ -275,7 +295,6 @@ void lane_main(tspg_server *S, int lane) {
   }
   tspg_batch_destroy(b1);
   tspg_batch_destroy(b2);
-  tspg_batch_destroy(bc);
 }
 
 }  // namespace
@@ -304,11 +323,15 @@ extern "C" int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
     S->lane_ctx.push_back(c);
     S->lane_stream.push_back(ls);
   }
+  if (st == TSPG_OK) st = tspg_ctx_create(dev, 0, &S->bctx);
+  if (st == TSPG_OK && cudaStreamCreateWithFlags(&S->bstream, cudaStreamNonBlocking) != cudaSuccess)
+    st = TSPG_ECUDA;
   if (st != TSPG_OK) {
     tspg_server_destroy(S);
     return st;
   }
   for (int l = 0; l < cfg->lanes; ++l) S->threads.emplace_back(lane_main, S, l);
+  S->threads.emplace_back(bound_main, S);
   *out = S;
   return TSPG_OK;
 }
@@ -319,6 +342,7 @@ extern "C" int tspg_server_destroy(tspg_server *S) {
     std::lock_guard<std::mutex> lk(S->mu);
     S->stop = true;
   }
+  S->cv_fresh.notify_all();
   S->cv_work.notify_all();
   for (auto &t : S->threads) t.join();
   cudaSetDevice(S->device);
@@ -332,12 +356,13 @@ extern "C" int tspg_server_destroy(tspg_server *S) {
     }
     delete r;
   }
-  for (Req *r : S->queue)
-    if (!S->reqs.count(r->ticket)) delete r;
+  // every request in fresh / queue is also in reqs (freed above)
   for (size_t l = 0; l < S->lane_ctx.size(); ++l) {
     if (S->lane_stream[l]) cudaStreamDestroy(S->lane_stream[l]);
     if (S->lane_ctx[l]) tspg_ctx_destroy(S->lane_ctx[l]);
   }
+  if (S->bstream) cudaStreamDestroy(S->bstream);
+  if (S->bctx) tspg_ctx_destroy(S->bctx);
   delete S;
   return TSPG_OK;
 }
@@ -362,9 +387,9 @@ extern "C" int tspg_server_submit(tspg_server *S, int kind, const tspg_csr *A,
   std::lock_guard<std::mutex> lk(S->mu);
   r->ticket = S->next_ticket++;
   S->reqs[r->ticket] = r;
-  S->queue.push_back(r);
+  S->fresh.push_back(r);
   *ticket = r->ticket;
-  S->cv_work.notify_one();
+  S->cv_fresh.notify_one();
   return TSPG_OK;
 }
 
@@ -429,7 +454,7 @@ extern "C" int tspg_server_stats(tspg_server *S, int64_t *batches, int64_t *comp
   std::lock_guard<std::mutex> lk(S->mu);
   if (batches) *batches = S->batches;
   if (completed) *completed = S->completed;
-  if (queued) *queued = int64_t(S->queue.size());
+  if (queued) *queued = int64_t(S->queue.size() + S->fresh.size());
   if (reserved) *reserved = S->reserved;
   return S->lane_error;
 }
