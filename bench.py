@@ -253,7 +253,8 @@ def run_ours(args, rank, world):
     bytes_c = csr_bytes(A.nrows, nnz_c, rp_bits // 8)
     algo = 2 * bytes_a + bytes_c
     sym, num = statistics.mean(sym_ms), statistics.mean(num_ms)
-    dom_ms, dom_name = (num, "k_phase<numeric>") if num >= sym else (sym, "k_phase<symbolic>")
+    dom_ms, dom_name = ((num, "numeric phase (k_phase + k_groups)") if num >= sym
+                        else (sym, "symbolic phase (k_phase + k_groups)"))
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -477,7 +478,7 @@ def run_batched(args):
     loop_ms = e0.elapsed_time(e1)
     n = len(dev)
     line = {
-        "metric": "batched products/s (512 independent FP64 A_i B_i, one persistent launch per phase)",
+        "metric": "batched products/s (512 independent FP64 A_i B_i, all in one launch of each persistent kernel per phase)",
         "value": round(n / (ms * 1e-3), 1), "unit": "products/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Poisson-row matrices, values U[-1,1])",

@@ -2,16 +2,16 @@
 // per phase.
 //
 // All rows of all products form one flat row space (row g of product p is
-// base[p] + r).  The same binning / persistent k_phase kernels as the single
+// base[p] + r).  The same binning / persistent kernels as the single
 // product path run once over that space, so the device work queue interleaves
 // rows of every product, heaviest class first; a product of 1k rows and one of
 // 200k rows cost one launch each phase together.  Outputs land in one slab
 // (int32 columns, values, int64 row offsets with one extra entry per product).
 //
 // A run is two CUDA graphs around one host sync (the output size):
-//   graph 1: sortedness check, mults, binning, symbolic k_phase, scan,
+//   graph 1: sortedness check, mults, binning, symbolic k_phase + k_groups, scan,
 //            per-product offsets -> pinned host;
-//   graph 2: output pointers, numeric binning, numeric k_phase.
+//   graph 2: output pointers, numeric binning, numeric k_phase + k_groups.
 // The graphs are captured on the first run and replayed while the batch's
 // operands are unchanged; tspg_batch_add / clear drop them.
 #include <cstring>

@@ -97,7 +97,8 @@ constexpr int kErrWord = 0;  // device-side error code (0 = ok)
     if (_s != TSPG_OK) return _s;     \
   } while (0)
 
-// Event pair k (0: symbolic phase, 1: numeric phase) around a k_phase launch.
+// Event pair k (0: symbolic phase, 1: numeric phase) around the two persistent
+// kernels of a phase (k_phase, then k_groups).
 inline void phase_mark(tspg_ctx *ctx, int k, int edge, cudaStream_t s) {
   if (!ctx->phase_timing) return;
   cudaEventRecord(ctx->ev[2 * k + edge], s);

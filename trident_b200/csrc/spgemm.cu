@@ -2,9 +2,9 @@
 //
 // Call sequence of one product on the caller's stream:
 //   k_set_prod, [k_check_sorted_rows], k_row_mults, k_sched_offsets,
-//   k_scatter<sym>, k_phase<symbolic>, k_scan_reduce / k_scan_partials /
+//   k_scatter<sym>, k_phase + k_groups <symbolic>, k_scan_reduce / k_scan_partials /
 //   k_scan_final, one 2-word device->host read + stream sync (nnz(C), longest
-//   A row), then k_set_out, k_sched_offsets, k_scatter<num>, k_phase<numeric>.
+//   A row), then k_set_out, k_sched_offsets, k_scatter<num>, k_phase + k_groups <numeric>.
 // KokkosSparse::spgemm (include/KokkosWrap.hpp:375) and the cuSPARSE paths
 // (include/cusparse_helpers.cuh:908-1344) do the same job with library-owned
 // allocation and ~10 stream syncs per call.

@@ -339,7 +339,7 @@ __all__ = ["Context", "Plan", "spgemm", "spgemm_count", "spgemm_count_mask", "sp
 
 
 class Batch:
-    """Many independent products in one persistent launch per phase
+    """Many independent products in one launch of each persistent kernel per phase
     (tspg_batch_*).  Operands are borrowed: keep the DeviceCSR objects alive."""
 
     def __init__(self, ctx: Context):
