@@ -168,3 +168,41 @@ def test_coo_to_csx_follows_reference_steps():
     # equal coordinates keep their input order
     pos = np.lexsort((np.arange(nnz), c, r))
     np.testing.assert_array_equal(oval, v[pos])
+
+
+def test_mcl_updates_follow_reference_loops():
+    # prune / normalize / inflation of the reference's MCL driver, written out
+    # as its host loops (row by row, in entry order) in plain Python
+    rng = np.random.default_rng(12)
+    n = 30
+    rowptr = [0]
+    col, val = [], []
+    for i in range(n):
+        k = int(rng.integers(0, 6))
+        cs = sorted(rng.choice(n, k, replace=False).tolist())
+        col += cs
+        val += rng.uniform(0, 1, k).tolist()
+        rowptr.append(len(col))
+    val[rowptr[3]:rowptr[4]] = [0.0] * (rowptr[4] - rowptr[3])  # a row summing to 0
+
+    def normalize(v):
+        out = list(v)
+        for i in range(n):
+            s = sum(v[rowptr[i]:rowptr[i + 1]])
+            for j in range(rowptr[i], rowptr[i + 1]):
+                out[j] = v[j] / s if s > 1e-20 else 0.0
+        return out
+
+    want = normalize([x ** 2.0 for x in val])
+    np.testing.assert_allclose(oracle.mcl_inflate(rowptr, val, 2.0), want, rtol=1e-14)
+    np.testing.assert_allclose(oracle.mcl_normalize(rowptr, val), normalize(val), rtol=1e-14)
+    tol = 0.3
+    prp, pcol, pval = [0], [], []
+    for i in range(n):
+        for j in range(rowptr[i], rowptr[i + 1]):
+            if abs(val[j]) > tol:
+                pcol.append(col[j])
+                pval.append(val[j])
+        prp.append(len(pcol))
+    grp, gcol, gval = oracle.mcl_prune(rowptr, col, val, tol)
+    assert grp.tolist() == prp and gcol.tolist() == pcol and gval.tolist() == pval
