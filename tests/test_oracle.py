@@ -206,3 +206,22 @@ def test_mcl_updates_follow_reference_loops():
         prp.append(len(pcol))
     grp, gcol, gval = oracle.mcl_prune(rowptr, col, val, tol)
     assert grp.tolist() == prp and gcol.tolist() == pcol and gval.tolist() == pval
+
+
+def test_summa_tiles_cover_the_matrix():
+    # the host-side q x q tile cut of the SUMMA emulation: every entry lands in
+    # exactly one tile, rebased, and the tiles put back together give the matrix
+    import scipy.sparse as sp
+    from trident_b200 import summa
+    A = workloads.rmat(scale=9, edge_factor=8, seed=4)
+    q = 4
+    tiles, rb, cb = summa.cut_tiles(A, q)
+    assert rb[0] == cb[0] == 0 and rb[-1] == A.nrows and cb[-1] == A.ncols
+    blocks = [[sp.csr_matrix((t.val, t.col, t.rowptr), shape=(rb[i + 1] - rb[i], cb[j + 1] - cb[j]))
+               for j, t in enumerate(row)] for i, row in enumerate(tiles)]
+    M = sp.bmat(blocks, format="csr")
+    M.sort_indices()
+    assert sum(t.nnz for row in tiles for t in row) == A.nnz
+    np.testing.assert_array_equal(M.indptr, A.rowptr)
+    np.testing.assert_array_equal(M.indices, A.col)
+    np.testing.assert_array_equal(M.data, A.val)
