@@ -54,7 +54,6 @@ def parse():
     p.add_argument("--scale", type=int, default=20)
     p.add_argument("--edge-factor", type=int, default=16)
     p.add_argument("--seed", type=int, default=1)
-    p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -117,6 +116,7 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workload
 def make_workload(args):
+    """The operand and the workload description shared by both arms' `config`."""
     from trident_b200 import workloads
     if args.workload == "rmat":
         A = workloads.rmat(scale=args.scale, edge_factor=args.edge_factor, seed=args.seed)
@@ -125,40 +125,89 @@ def make_workload(args):
     else:
         A = workloads.uniform_rows(1024, 16, True, seed=args.seed)
         cfg = {"workload": "uniform1024_AxA", "rows": A.nrows, "nnz_A": A.nnz, "seed": args.seed}
+    a_bytes = csr_bytes(A.nrows, A.nnz, 4)
+    cfg["l2"] = ("inputs and outputs larger than L2 (A %.0f MB; C holds at least nnz(A) entries)" % (a_bytes / 1e6)
+                 if a_bytes > L2_BYTES else "A fits L2 (launch-bound case)")
     return A, cfg
 
 
-def cpu_baseline(A, mults_total, seconds):
-    """Oracle (CPU restatement, all host threads) on a strided row sample."""
+def sample_rows(A, mults_total, target=2.5e9):
+    """The CPU sample of a workload: rows i = 1 mod s of A (all rows when
+    s = 1), s the smallest power of two that keeps the sample at or below
+    `target` multiply-adds (about 5 s of the oracle on 16 host cores).  The
+    timed CPU baseline, the reference arm and the parity check all use it."""
     import numpy as np
+    s = 1
+    while mults_total / s > target:
+        s *= 2
+    return s, np.arange(1 if s > 1 else 0, A.nrows, s, dtype=np.int64)
 
+
+def cpu_baseline(A, rows, stride, rm):
+    """Oracle (CPU restatement, all host threads) on the sample rows of A·A."""
     import oracle
-    from trident_b200.csr import HostCSR
-    rm = oracle.row_mults(A, A)
-    # calibrate: time a small sample, then size the real one to ~`seconds`
-    def sample(stride, offset=0):
-        rows = np.arange(offset, A.nrows, stride)
-        rp = np.zeros(rows.size + 1, dtype=np.int64)
-        rp[1:] = np.cumsum(A.rowptr[rows + 1] - A.rowptr[rows])
-        idx = np.concatenate([np.arange(A.rowptr[r], A.rowptr[r + 1]) for r in rows]) if rows.size else \
-            np.zeros(0, np.int64)
-        return HostCSR(rows.size, A.ncols, rp, A.col[idx], A.val[idx]), int(rm[rows].sum())
-
-    stride = max(1, int(2 ** math.ceil(math.log2(max(1.0, mults_total / 2e8)))))
-    S, mu = sample(stride)
-    t0 = time.perf_counter()
-    oracle.spgemm(S, A, with_abs=False)
-    dt = time.perf_counter() - t0
-    rate = mu / max(dt, 1e-6)
-    want = rate * seconds
-    stride2 = max(1, int(round(mults_total / max(want, 1.0))))
-    S, mu = sample(stride2, offset=1)
+    S = A.rows(rows)
+    mu = int(rm[rows].sum())
     t0 = time.perf_counter()
     oracle.spgemm(S, A, with_abs=False)
     dt = time.perf_counter() - t0
     return {"value": round(2 * mu / dt / 1e9, 4), "unit": "GFLOP/s", "cores": oracle.num_threads(),
-            "kind": "port",
-            "sample": f"rows i = 1 mod {stride2} of A times A ({S.nrows} rows, {mu} mults, {dt:.1f} s)"}
+            "kind": "port", "ms": round(dt * 1e3, 1),
+            "sample": f"rows i = 1 mod {stride} of A times A ({S.nrows} rows, {mu} mults)"
+            if stride > 1 else f"all rows of A times A ({S.nrows} rows, {mu} mults)"}
+
+
+def gather_rows(Crp, Ccol, Cval, rows):
+    """Rows `rows` (numpy int64, ascending) of a device CSR, copied to the host:
+    (row lengths, columns, values)."""
+    import numpy as np
+    import torch
+    rr = torch.from_numpy(rows).to(Crp.device)
+    starts = Crp[rr].to(torch.int64)
+    lens = Crp[rr + 1].to(torch.int64) - starts
+    tot = int(lens.sum().item())
+    if tot == 0:
+        return lens.cpu().numpy(), np.zeros(0, np.int32), np.zeros(0, np.float64)
+    excl = torch.cumsum(lens, 0) - lens
+    idx = torch.repeat_interleave(starts - excl, lens) + torch.arange(tot, device=Crp.device)
+    cols, vals = Ccol[idx].cpu().numpy(), Cval[idx].cpu().numpy()
+    del idx
+    return lens.cpu().numpy(), cols, vals
+
+
+def parity_rows(A, B, rows, Crp, Ccol, Cval, chunk=150_000_000):
+    """Rows `rows` of the GPU's C = A·B against the oracle: row lengths and
+    sorted columns bit-exact, values within 1e-12 * max(|y|, sum |a_ik b_kj|).
+    Chunked by output entries so host and device memory stay bounded."""
+    import numpy as np
+    import oracle
+    import torch
+    TOL = 1e-12
+    rr = torch.from_numpy(rows).to(Crp.device)
+    lens_all = (Crp[rr + 1].to(torch.int64) - Crp[rr].to(torch.int64)).cpu().numpy()
+    cum = np.cumsum(lens_all)
+    cuts = [0]
+    while cuts[-1] < rows.size:
+        base = cum[cuts[-1] - 1] if cuts[-1] else 0
+        nxt = int(np.searchsorted(cum, base + chunk, side="right"))
+        cuts.append(min(rows.size, max(nxt, cuts[-1] + 1)))
+    ok, worst, nnz = True, 0.0, 0
+    for c0, c1 in zip(cuts[:-1], cuts[1:]):
+        sub = rows[c0:c1]
+        lens, cols, vals = gather_rows(Crp, Ccol, Cval, sub)
+        rp, cj, cx, ca = oracle.spgemm(A.rows(sub), B, with_abs=True)
+        if not (np.array_equal(lens, np.diff(rp)) and np.array_equal(cols, cj)):
+            ok = False
+            break
+        if cx.size:
+            rel = np.abs(vals - cx) / np.maximum(np.maximum(np.abs(cx), ca), 1e-300)
+            worst = max(worst, float(rel.max()))
+        nnz += int(cx.size)
+    rowptr_ok = bool(int(Crp[0].item()) == 0 and bool((Crp[1:] >= Crp[:-1]).all().item()))
+    return {"rows_checked": int(rows.size), "entries_checked": nnz, "structure_equal": bool(ok),
+            "rowptr_monotone": rowptr_ok, "max_rel_err": worst, "tolerance": TOL,
+            "values_within_tolerance": bool(ok and worst <= TOL),
+            "rule": "row lengths and columns bit-exact; |x - y| <= 1e-12 * max(|y|, sum |a_ik b_kj|)"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -191,8 +240,7 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     A, cfg = make_workload(args)
     ctx = ops.Context(dev)
-    if args.workload == "rmat":
-        cfg["tuning"] = apply_tuning(ctx, "rmat")
+    cfg_tuning = apply_tuning(ctx, "rmat") if args.workload == "rmat" else None
     dA = A.to_device(rowptr_bits=32)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
@@ -277,17 +325,25 @@ def run_ours(args, rank, world):
     if not args.no_e2e:
         e2e = run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, (Crp, Ccol, Cval))
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(A, mults, args.cpu_seconds)
+        import oracle
+        rm = oracle.row_mults(A, A)
+        stride, rows = sample_rows(A, mults)
+        cpu = cpu_baseline(A, rows, stride, rm)
+        # the same rows of the GPU's C (the last timed call's output) against the oracle
+        parity = parity_rows(A, A, rows, Crp, Ccol, Cval)
+        parity["sample"] = cpu["sample"]
 
     line = {
         "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64",
         "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
-        "config": dict(cfg, mults=mults, nnz_C=nnz_c, c_rowptr_bits=rp_bits, parallelism=f"replicas{world}",
-                       l2="inputs and outputs larger than L2 (A %.0f MB, C %.0f MB)" % (bytes_a / 1e6, bytes_c / 1e6)),
+        "config": dict(cfg, mults=mults),
+        "parallelism": f"replicas{world}",
+        "output": {"nnz_C": nnz_c, "c_rowptr_bits": rp_bits, "C_MB": round(bytes_c / 1e6)},
+        "tuning": cfg_tuning,
         "phase_ms": {"symbolic": round(sym, 3), "numeric": round(num, 3)},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
                      "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
@@ -300,6 +356,7 @@ def run_ours(args, rank, world):
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "parity": parity,
     }
     ctx.close()
     return line
@@ -385,26 +442,29 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
 def run_reference(args):
     """The reference's CPU path for the same product: the oracle restatement
     of KokkosKernels SpGEMM semantics (KokkosKernels itself is not vendored
-    and cannot be built here), all host threads, bounded row samples."""
-    import time as _t
-
+    and cannot be built here), all host threads.  Every step multiplies the
+    same row sample as the GPU arm's cpu_baseline leg (rows i = 1 mod s of
+    A·A); the operand comes from the host-only generator library, so this arm
+    maps no device code."""
     import oracle
     A, cfg = make_workload(args)
     rm = oracle.row_mults(A, A)
     mults = int(rm.sum())
-    vals = []
-    per = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    stride, rows = sample_rows(A, mults)
+    times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(A, mults, per)
+        r = cpu_baseline(A, rows, stride, rm)
         if i >= args.warmup:
-            vals.append(r)
-    v = statistics.mean(x["value"] for x in vals)
+            times.append(r["ms"])
+    ms = statistics.mean(times)
+    mu = int(rm[rows].sum())
+    v = 2 * mu / (ms * 1e-3) / 1e9
     return {"impl": "reference", "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64", "value": round(v, 4),
-            "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
-            "config": dict(cfg, mults=mults),
-            "cpu_baseline": {"value": round(v, 4), "unit": "GFLOP/s", "cores": vals[-1]["cores"], "kind": "port",
-                             "sample": vals[-1]["sample"]},
+            "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded R-MAT, values U[-1,1])", "config": dict(cfg, mults=mults),
+            "cpu_baseline": {"value": round(v, 4), "unit": "GFLOP/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
             "e2e": {"value": round(v, 4), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -453,6 +513,28 @@ def run_batched(args):
     l1 = C.c_int64()
     lib.tspg_ctx_stats(ctx.h, C.byref(l1))
     ms = e0.elapsed_time(e1) / args.steps
+    # parity: a seeded subset of the products (results of the last timed run)
+    # against the oracle, and the oracle's time on them as the CPU baseline
+    import oracle
+    pick = sorted(int(i) for i in np.random.default_rng(args.seed).choice(len(dev), size=min(8, len(dev)),
+                                                                             replace=False))
+    checks, cpu_s, cpu_mults = [], 0.0, 0
+    for i in pick:
+        Ai, Bi = workloads.batched_product(specs[i])
+        Ri = bt.result(i)
+        checks.append(parity_rows(Ai, Bi, np.arange(Ai.nrows, dtype=np.int64), Ri.rowptr, Ri.col, Ri.val))
+        t0 = time.perf_counter()
+        oracle.spgemm(Ai, Bi, with_abs=False)
+        cpu_s += time.perf_counter() - t0
+        cpu_mults += int(oracle.row_mults(Ai, Bi).sum())
+    parity = {"products_checked": pick, "entries_checked": sum(c["entries_checked"] for c in checks),
+              "structure_equal": all(c["structure_equal"] for c in checks),
+              "max_rel_err": max(c["max_rel_err"] for c in checks), "tolerance": 1e-12,
+              "values_within_tolerance": all(c["values_within_tolerance"] for c in checks)}
+    mean_mults = mults / len(dev)
+    cpu = {"value": round(cpu_mults / cpu_s / mean_mults, 2), "unit": "products/s", "cores": oracle.num_threads(),
+           "kind": "port", "sample": f"products {pick} ({cpu_mults} mults, {cpu_s:.2f} s), scaled to the mean "
+                                     f"product of the batch ({mean_mults:.0f} mults)"}
     # the same products as a loop of plain calls (output buffer reused)
     maxnnz = max(int(bt.result(i).nnz) for i in range(len(dev)))
     maxrows = max(dA.nrows for dA, _ in dev)
@@ -490,6 +572,8 @@ def run_batched(args):
         "speedup_vs_loop": round(loop_ms / ms, 3),
         "gpu_launches": int(l1.value - l0.value),
         "clocks": clk,
+        "cpu_baseline": cpu,
+        "parity": parity,
     }
     bt.close()
     ctx.close()
@@ -499,11 +583,14 @@ def run_batched(args):
 def run_rap(args):
     """AMG Galerkin product on the 27-point Laplacian of an n^3 grid (n = 128 by
     default, --scale sets n): AP = A·P, then RAP = R·(AP), R = P^T built by an
-    untimed host transpose.  One step = both products."""
+    untimed host transpose.  One step = both products.  Parity: the whole AP
+    and RAP against the oracle; CPU baseline: the oracle on both products."""
     import ctypes as C
 
+    import numpy as np
     import torch
 
+    import oracle
     from trident_b200 import ops, workloads
     from trident_b200._lib import TSPG_F_B_SORTED, TspgCsrOut, check, lib
     n = args.scale if args.scale != 20 else 128
@@ -527,39 +614,78 @@ def run_rap(args):
         check(lib.tspg_spgemm(ctx.h, stream.cuda_stream, C.byref(x), C.byref(y), C.byref(o), TSPG_F_B_SORTED),
               "tspg_spgemm")
 
-    def step():
+    for _ in range(max(args.warmup, 3)):
         call(dA, dP, AP)
         call(dR, AP, RAP)
-
-    for _ in range(args.warmup):
-        step()
     torch.cuda.synchronize()
+    check(lib.tspg_ctx_phase_timing(ctx.h, 1), "phase timing")
+    l0 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(l0))
+    clocks = ClockSampler(0)
+    clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_ap = 0.0
+    fs, fn = C.c_float(), C.c_float()
+    num = {"AP": [], "RAP": []}
     e0.record(stream)
     for _ in range(args.steps):
         ea.record(stream)
         call(dA, dP, AP)
         eb.record(stream)
+        lib.tspg_ctx_phase_ms(ctx.h, C.byref(fs), C.byref(fn))
+        num["AP"].append(fn.value)
         call(dR, AP, RAP)
-        torch.cuda.synchronize()
+        lib.tspg_ctx_phase_ms(ctx.h, C.byref(fs), C.byref(fn))
+        num["RAP"].append(fn.value)
         t_ap += ea.elapsed_time(eb)
     e1.record(stream)
     torch.cuda.synchronize()
+    clk = clocks.stop()
+    check(lib.tspg_ctx_phase_timing(ctx.h, 0), "phase timing")
+    l1 = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(l1))
     ms = e0.elapsed_time(e1) / args.steps
     ap_ms = t_ap / args.steps
     peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
     bap = csr_bytes(A.nrows, A.nnz, 4) + csr_bytes(P.nrows, P.nnz, 4) + csr_bytes(AP.nrows, AP.nnz, 4)
     brap = csr_bytes(R.nrows, R.nnz, 4) + csr_bytes(AP.nrows, AP.nnz, 4) + csr_bytes(RAP.nrows, RAP.nnz, 4)
+    ap_num = statistics.mean(num["AP"])
+    rap_num = statistics.mean(num["RAP"])
+    # CPU baseline: the oracle on both products, timed
+    from trident_b200.synth import HostCSR
+    t0 = time.perf_counter()
+    orp, oj, ox, _ = oracle.spgemm(A, P, with_abs=False)
+    Ho = HostCSR(A.nrows, P.ncols, orp, oj, ox)
+    oracle.spgemm(R, Ho, with_abs=False)
+    cpu_s = time.perf_counter() - t0
+    # parity: the whole AP and RAP of the last timed step against the oracle
+    # (RAP = R times the oracle's own AP)
+    parity = {name: parity_rows(X, Y, np.arange(X.nrows, dtype=np.int64), G.rowptr, G.col, G.val)
+              for name, X, Y, G in (("AP", A, P, AP), ("RAP", R, Ho, RAP))}
     line = {
         "metric": "Galerkin R·A·P GFLOP/s (2 x multiply-adds), FP64", "value": round(2.0 * (m1 + m2) / (ms * 1e-3) / 1e9, 3),
-        "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-        "higher_is_better": True, "dtype": "f64", "data": "synthetic (27-point Laplacian, SA prolongator)",
-        "config": {"tuning": tuning, "workload": f"rap27pt_{n}^3", "nnz_A": A.nnz, "nnz_P": P.nnz, "nnz_AP": AP.nnz, "nnz_RAP": RAP.nnz,
-                   "mults_AP": int(m1), "mults_RAP": int(m2)},
-        "AP": {"ms": round(ap_ms, 3), "hbm_frac": round(bap / (ap_ms * 1e-3) / 1e9 / peak, 4)},
-        "RAP": {"ms": round(ms - ap_ms, 3), "hbm_frac": round(brap / ((ms - ap_ms) * 1e-3) / 1e9 / peak, 4)},
+        "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (27-point Laplacian, SA prolongator)",
+        "config": {"workload": f"rap27pt_{n}^3", "nnz_A": A.nnz, "nnz_P": P.nnz, "nnz_AP": AP.nnz,
+                   "nnz_RAP": RAP.nnz, "mults_AP": int(m1), "mults_RAP": int(m2),
+                   "l2": "A (%.0f MB) larger than L2; P, AP, RAP re-read from L2/HBM" % (csr_bytes(A.nrows, A.nnz, 4) / 1e6)},
+        "tuning": tuning,
+        "AP": {"ms": round(ap_ms, 3), "numeric_ms": round(ap_num, 3),
+               "hbm_frac": round(bap / (ap_ms * 1e-3) / 1e9 / peak, 4)},
+        "RAP": {"ms": round(ms - ap_ms, 3), "numeric_ms": round(rap_num, 3),
+                "hbm_frac": round(brap / ((ms - ap_ms) * 1e-3) / 1e9 / peak, 4)},
+        "roofline": {"bound": "hbm", "kernel": "numeric phase of A·P (k_phase + k_groups)",
+                     "achieved": round(bap / (ap_num * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(bap / (ap_num * 1e-3) / 1e9 / peak, 4), "traffic": None,
+                     "algorithmic_bytes": bap},
+        "gpu_launches": int(l1.value - l0.value),
+        "clocks": clk,
+        "cpu_baseline": {"value": round(2.0 * (m1 + m2) / cpu_s / 1e9, 4), "unit": "GFLOP/s",
+                         "cores": oracle.num_threads(), "kind": "port",
+                         "sample": f"the whole workload (A·P then R·AP), {cpu_s:.2f} s"},
+        "parity": parity,
     }
     ctx.close()
     return line

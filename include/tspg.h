@@ -300,8 +300,10 @@ int tspg_pack(tspg_ctx *ctx, void *stream, const tspg_csr *M, int major,
  * 3 MiB per GPU, held until exit) sized for tiles of up to
  * TSPG_PACK_NOALLOC_MAX_SEGMENTS segments; larger tiles return
  * TSPG_ESCRATCH.  The first call on a device looks up that array's device
- * address (make it before any stream capture).  All calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * address (make it before any stream capture).  The device current on the
+ * calling thread must own `stream` and the buffers; an output buffer on
+ * another device returns TSPG_EINVAL.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 #define TSPG_PACK_NOALLOC_MAX_SEGMENTS 262144
 int tspg_pack_noalloc(void *stream, const tspg_csr *M, int major,
                       const uint8_t *mask, void *out_buf, size_t cap,
@@ -403,43 +405,6 @@ int tspg_server_wait(tspg_server *s, int64_t ticket, int timeout_ms,
 int tspg_server_release(tspg_server *s, int64_t ticket);
 int tspg_server_stats(tspg_server *s, int64_t *batches, int64_t *completed,
                       int64_t *queued, size_t *reserved);
-
-/* ---- synthetic inputs (host) -----------------------------------------------------
- * Seeded generators of the benchmark operands, host memory, int64 rowptr.
- * Arrays are allocated with malloc and released with tspg_host_free. */
-typedef struct tspg_host_csr {
-  int64_t nrows, ncols, nnz;
-  int64_t *rowptr;
-  int32_t *col;
-  double *val;
-} tspg_host_csr;
-void tspg_host_free(tspg_host_csr *M);
-/* n x n, row i = k distinct uniform columns plus (if diag) column i. */
-int tspg_gen_uniform_rows(int64_t n, int k, int diag, uint64_t seed,
-                          tspg_host_csr *out);
-/* R-MAT: 2^scale rows, edge_factor*2^scale draws, quadrant probabilities
- * a, b, c (d = 1-a-b-c), duplicates merged, self-loops kept. */
-int tspg_gen_rmat(int scale, int edge_factor, double a, double b, double c,
-                  uint64_t seed, tspg_host_csr *out);
-/* 27-point (pts=27, 26 / -1) or 7-point (pts=7, 6 / -1) Laplacian on an
- * nx*ny*nz grid, lexicographic x-fastest numbering. */
-int tspg_gen_laplacian(int64_t nx, int64_t ny, int64_t nz, int pts,
-                       tspg_host_csr *out);
-/* Smoothed-aggregation prolongator P = (I - omega D^-1 A) P_tent for a
- * Laplacian A from tspg_gen_laplacian, aggregates agg^3 by integer division
- * of the grid coordinates, P_tent 0/1 (unnormalised). */
-int tspg_gen_sa_prolongator(int64_t nx, int64_t ny, int64_t nz, int pts,
-                            int agg, double omega, tspg_host_csr *out);
-/* Host transpose (R = P^T for the Galerkin product). */
-int tspg_host_transpose(const tspg_host_csr *M, tspg_host_csr *out);
-/* Random square matrix of the batched workload: rows x rows, row lengths
- * Poisson(lambda), distinct uniform columns. */
-int tspg_gen_poisson_rows(int64_t rows, double lambda, uint64_t seed,
-                          tspg_host_csr *out);
-/* Read a Trident .bmtx file (MatrixMarket banner with index and value byte
- * widths, then little-endian (row, col, float32) records) into CSR with
- * duplicates kept in file order. */
-int tspg_read_bmtx(const char *path, tspg_host_csr *out);
 
 #ifdef __cplusplus
 }

@@ -1,9 +1,10 @@
 """Regenerate the golden fixtures of tests/golden/.
 
-Run from the repository root in a checkout that has the reference tree at
-/root/reference (the fixtures are committed, so tests never need it):
+Run from the repository root, naming the reference's small_matrices folder
+when the .bmtx fixtures should be refreshed from it (the fixtures are
+committed, so tests never need the reference tree):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--bmtx-dir <reference>/small_matrices]
 
 What it writes:
   * n16_full.bmtx, n1024.bmtx — the reference's own small_matrices fixtures
@@ -15,6 +16,7 @@ What it writes:
   * oracle_bmtx.json — digests of the oracle's A·A for the two fixtures, which
     pin the oracle's structure (and value sums) across machines.
 """
+import argparse
 import hashlib
 import json
 import os
@@ -25,7 +27,6 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference/small_matrices"
 
 
 def kats():
@@ -59,10 +60,13 @@ def digest(a):
 
 
 def main():
-    for f in ("n16_full.bmtx", "n1024.bmtx"):
-        src = os.path.join(REF, f)
-        if os.path.exists(src):
-            shutil.copyfile(src, os.path.join(HERE, f))
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--bmtx-dir", default=None,
+                    help="the reference's small_matrices folder to copy the .bmtx fixtures from")
+    args = ap.parse_args()
+    if args.bmtx_dir:
+        for f in ("n16_full.bmtx", "n1024.bmtx"):
+            shutil.copyfile(os.path.join(args.bmtx_dir, f), os.path.join(HERE, f))
     with open(os.path.join(HERE, "kat_bitmask.json"), "w") as fh:
         json.dump(kats(), fh, indent=1)
     sys.path.insert(0, ROOT)

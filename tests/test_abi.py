@@ -1,33 +1,47 @@
-"""CPU: the C-ABI library loads, exports every declared symbol, and its
-host-side pieces (generators, .bmtx reader, pack layout arithmetic) behave."""
+"""CPU: the C-ABI libraries load, export every symbol their headers declare,
+and their host-side pieces (generators, .bmtx reader, pack layout arithmetic)
+behave."""
 import ctypes as C
 import os
 import re
+import subprocess
+import sys
 
 import numpy as np
 import pytest
 
-from trident_b200 import _lib, workloads
+from trident_b200 import _lib, synth, workloads
 from trident_b200._lib import TspgCsr, lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLD = os.path.join(ROOT, "tests", "golden")
 
 
-def declared_symbols():
-    syms = set()
-    for name in os.listdir(os.path.join(ROOT, "include")):
-        if name.endswith(".h"):
-            text = open(os.path.join(ROOT, "include", name)).read()
-            syms |= set(re.findall(r"\b(tspg_[a-z0-9_]+)\s*\(", text))
-    return syms
+def declared_symbols(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    return set(re.findall(r"\b(tspg_[a-z0-9_]+)\s*\(", text))
 
 
 def test_every_declared_symbol_is_exported():
-    syms = declared_symbols()
-    assert len(syms) > 20
-    missing = [s for s in sorted(syms) if not hasattr(lib, s)]
-    assert not missing, missing
+    """Every C header under include/ is bound to the library that exports it."""
+    headers = {"tspg.h": lib, "tspg_synth.h": synth.lib}
+    assert sorted(n for n in os.listdir(os.path.join(ROOT, "include")) if n.endswith(".h")) == sorted(headers)
+    for header, library in headers.items():
+        syms = declared_symbols(header)
+        assert len(syms) > 5, header
+        missing = [s for s in sorted(syms) if not hasattr(library, s)]
+        assert not missing, (header, missing)
+    assert len(declared_symbols("tspg.h")) > 20
+
+
+def test_generators_do_not_map_the_device_library():
+    """The CPU legs of the benchmark build their operands through
+    trident_b200.workloads alone: that loads libtspg_synth.so, never libtspg.so."""
+    code = ("import sys; sys.path.insert(0, %r); import trident_b200.workloads as w; "
+            "w.rmat(scale=8); m = open('/proc/self/maps').read(); "
+            "print(int('libtspg.so' in m), int('libtspg_synth.so' in m))" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout.split()
+    assert out == ["0", "1"]
 
 
 def test_abi_version_and_strerror():

@@ -68,17 +68,6 @@ class TspgServerConfig(C.Structure):
 TSPG_REQ_AB, TSPG_REQ_RAP = 0, 1
 
 
-class TspgHostCsr(C.Structure):
-    _fields_ = [
-        ("nrows", C.c_int64),
-        ("ncols", C.c_int64),
-        ("nnz", C.c_int64),
-        ("rowptr", C.POINTER(C.c_int64)),
-        ("col", C.POINTER(C.c_int32)),
-        ("val", C.POINTER(C.c_double)),
-    ]
-
-
 class TspgError(RuntimeError):
     def __init__(self, status: int, what: str):
         self.status = status
@@ -139,14 +128,6 @@ def _load() -> C.CDLL:
         "tspg_server_wait": (i32, [vp, i64, i32, P(TspgCsr), P(C.c_double)]),
         "tspg_server_release": (i32, [vp, i64]),
         "tspg_server_stats": (i32, [vp, P(i64), P(i64), P(i64), P(sz)]),
-        "tspg_host_free": (None, [P(TspgHostCsr)]),
-        "tspg_gen_uniform_rows": (i32, [i64, i32, i32, C.c_uint64, P(TspgHostCsr)]),
-        "tspg_gen_rmat": (i32, [i32, i32, C.c_double, C.c_double, C.c_double, C.c_uint64, P(TspgHostCsr)]),
-        "tspg_gen_laplacian": (i32, [i64, i64, i64, i32, P(TspgHostCsr)]),
-        "tspg_gen_sa_prolongator": (i32, [i64, i64, i64, i32, i32, C.c_double, P(TspgHostCsr)]),
-        "tspg_host_transpose": (i32, [P(TspgHostCsr), P(TspgHostCsr)]),
-        "tspg_gen_poisson_rows": (i32, [i64, C.c_double, C.c_uint64, P(TspgHostCsr)]),
-        "tspg_read_bmtx": (i32, [C.c_char_p, P(TspgHostCsr)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

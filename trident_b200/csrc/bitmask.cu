@@ -152,6 +152,9 @@ extern "C" int tspg_pack(tspg_ctx *ctx, void *stream, const tspg_csr *M,
   TSPG_TRY(check_csr(M));
   if (major != TSPG_ROWS && major != TSPG_COLS) return TSPG_EINVAL;
   const int64_t len = major == TSPG_ROWS ? M->nrows : M->ncols;
+  // the pointer array has len + 1 entries: no segments means no entries, and
+  // a non-empty pointer array must be given
+  if ((len == 0 && M->nnz > 0) || (len > 0 && !M->rowptr)) return TSPG_EINVAL;
   if (len > 0 && !mask) return TSPG_EINVAL;
   if ((uintptr_t)out_buf & 7) return TSPG_EINVAL;
   if (cap < tspg_packed_bytes(M->nnz, len, M->val_bits, M->rowptr_bits)) return TSPG_ENOMEM;

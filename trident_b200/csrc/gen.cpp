@@ -16,7 +16,7 @@
 #include <omp.h>
 #endif
 
-#include "tspg.h"
+#include "tspg_synth.h"
 
 namespace {
 

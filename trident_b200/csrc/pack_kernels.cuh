@@ -33,7 +33,8 @@ __global__ void __launch_bounds__(256)
                 int64_t *kept_dev) {
   using V = typename std::conditional<VB == 8, unsigned long long, unsigned>::type;
   const int64_t kept = newp[len];
-  const int64_t nnz = ptr[len];
+  // an empty pointer array (len == 0) may be null and holds no entries
+  const int64_t nnz = len > 0 ? int64_t(ptr[len]) : 0;
   V *oval = (V *)out;
   int32_t *oidx = (int32_t *)(out + kept * VB);
   const V *ival = (const V *)val;

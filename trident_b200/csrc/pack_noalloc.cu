@@ -17,7 +17,10 @@
 // TSPG_ESCRATCH.  Host code cannot use the array's name as a device address,
 // so on the first call on each device (with that device current) the entry
 // point asks the runtime for the address with cudaGetSymbolAddress and caches
-// it; make that first call before any stream capture.  All calls share the
+// it, with the device's SM count; make that first call before any stream
+// capture.  The device that is current on the calling thread must be the one
+// that owns the stream and the buffers: a call whose output buffer lives on
+// another device is rejected with TSPG_EINVAL.  All calls share the
 // array and it keeps the previous call's contents: the kernels write every
 // scratch word they read except the first pointer offset, which is cleared by
 // a kernel at the start of each call.  Calls whose kernels overlap on the GPU
@@ -44,25 +47,37 @@ __device__ __align__(256) unsigned char g_pack_scratch[kNoallocScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void *g_scratch_addr[kMaxDevices] = {};
+int g_num_sms[kMaxDevices] = {};
 
-// Device address of g_pack_scratch on the current device (set up once per
-// device).
-int scratch_for_current_device(void **out) {
+// Device address of g_pack_scratch on the current device and that device's
+// SM count (looked up once per device).  `probe` is a device buffer of the
+// call: when it belongs to another device the call is rejected.
+int scratch_for_current_device(const void *probe, void **out, int *num_sms) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     (void)cudaGetLastError();
     return TSPG_ECUDA;
   }
+  cudaPointerAttributes pa{};
+  if (cudaPointerGetAttributes(&pa, probe) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return TSPG_EINVAL;
+  }
+  if (pa.type == cudaMemoryTypeDevice && pa.device != dev) return TSPG_EINVAL;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_addr[dev]) {
     void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_pack_scratch) != cudaSuccess || !p) {
+    int sms = 0;
+    if (cudaGetSymbolAddress(&p, g_pack_scratch) != cudaSuccess || !p ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
       (void)cudaGetLastError();
       return TSPG_ECUDA;
     }
+    g_num_sms[dev] = sms > 0 ? sms : 1;
     g_scratch_addr[dev] = p;
   }
   *out = g_scratch_addr[dev];
+  *num_sms = g_num_sms[dev];
   return TSPG_OK;
 }
 
@@ -71,7 +86,7 @@ __global__ void k_clear_first(int64_t *newp) { newp[0] = 0; }
 template <typename PT>
 int pack_noalloc_impl(cudaStream_t s, const tspg_csr *M, int64_t len,
                       const uint8_t *mask, void *out_buf, int64_t *kept_dev,
-                      unsigned char *scratch) {
+                      unsigned char *scratch, int num_sms) {
   int32_t *cnt = (int32_t *)scratch;
   int64_t *newp = (int64_t *)(scratch + kOffNewp);
   int64_t *partial = (int64_t *)(scratch + kOffPartial);
@@ -88,7 +103,7 @@ int pack_noalloc_impl(cudaStream_t s, const tspg_csr *M, int64_t len,
   }
   const int64_t work = (M->nnz + kPackItems - 1) / kPackItems;
   const int64_t w = work > len + 1 ? work : len + 1;
-  const unsigned grid = (unsigned)std::min<int64_t>((w + 255) / 256, 148 * 32);
+  const unsigned grid = (unsigned)std::min<int64_t>((w + 255) / 256, int64_t(num_sms) * 32);
   if (M->val_bits == 64)
     k_pack_copy<PT, 8><<<grid, 256, 0, s>>>(ptr, len, M->col, M->val, mask, newp,
                                             (char *)out_buf, kept_dev);
@@ -112,15 +127,19 @@ extern "C" int tspg_pack_noalloc(void *stream, const tspg_csr *M, int major,
   if (major != TSPG_ROWS && major != TSPG_COLS) return TSPG_EINVAL;
   const int64_t len = major == TSPG_ROWS ? M->nrows : M->ncols;
   if (len > kNoallocMaxSeg) return TSPG_ESCRATCH;
+  // the pointer array has len + 1 entries: no segments means no entries, and
+  // a non-empty pointer array must be given
+  if ((len == 0 && M->nnz > 0) || (len > 0 && !M->rowptr)) return TSPG_EINVAL;
   if (len > 0 && !mask) return TSPG_EINVAL;
   if ((uintptr_t)out_buf & 7) return TSPG_EINVAL;
   if (cap < tspg_packed_bytes(M->nnz, len, M->val_bits, M->rowptr_bits)) return TSPG_ENOMEM;
   void *scratch = nullptr;
-  TSPG_TRY(scratch_for_current_device(&scratch));
+  int num_sms = 1;
+  TSPG_TRY(scratch_for_current_device(out_buf, &scratch, &num_sms));
   cudaStream_t s = (cudaStream_t)stream;
   if (M->rowptr_bits == 32)
     return pack_noalloc_impl<int32_t>(s, M, len, mask, out_buf, nnz_kept_dev,
-                                      (unsigned char *)scratch);
+                                      (unsigned char *)scratch, num_sms);
   return pack_noalloc_impl<int64_t>(s, M, len, mask, out_buf, nnz_kept_dev,
-                                    (unsigned char *)scratch);
+                                    (unsigned char *)scratch, num_sms);
 }

@@ -15,10 +15,15 @@
 
 namespace tspg {
 
+// The dynamic shared-memory limit is a per-device attribute of a kernel: it
+// is raised once per device (the caller has made ctx->device current), so a
+// process that drives several GPUs sets it on each of them.
 template <typename PT, typename VT>
-static int set_smem_attr() {
-  static bool done = false;  // per instantiation; benign if raced
-  if (!done) {
+static int set_smem_attr(int device) {
+  constexpr int kMaxDev = 64;
+  static bool done[kMaxDev] = {};  // per device and instantiation; benign if raced
+  const bool cached = device >= 0 && device < kMaxDev;
+  if (!cached || !done[device]) {
     cudaError_t e1 = cudaFuncSetAttribute(k_phase<PT, VT, false>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kDynSmem);
@@ -33,7 +38,7 @@ static int set_smem_attr() {
                                           kGroupDynSmem);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
       return TSPG_ECUDA;
-    done = true;
+    if (cached) done[device] = true;
   }
   return TSPG_OK;
 }
@@ -95,7 +100,7 @@ static inline unsigned grid_for(int64_t work, int per_block, int cap) {
 template <typename PT, typename VT>
 static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                          const tspg_csr *B, int flags, tspg_plan *P) {
-  TSPG_TRY(set_smem_attr<PT, VT>());
+  TSPG_TRY(set_smem_attr<PT, VT>(ctx->device));
   const int64_t m = A->nrows, n = B->ncols, k = A->ncols;
   P->m = m;
   P->n = n;

@@ -13,7 +13,8 @@ of the five workloads:
 * ``poisson_rows``  square random matrices with Poisson row lengths (batched
                     and served A·B requests)
 
-Values are uniform in [-1, 1] (FP64) except the stencil operators.
+Values are uniform in [-1, 1] (FP64) except the stencil operators.  Only the
+host-only generator library (libtspg_synth.so) is loaded here.
 """
 from __future__ import annotations
 
@@ -22,8 +23,7 @@ import math
 
 import numpy as np
 
-from ._lib import TspgHostCsr, check, lib
-from .csr import HostCSR
+from .synth import HostCSR, TspgHostCsr, check, lib
 
 
 def _gen(fn, *args) -> HostCSR:
