@@ -309,6 +309,26 @@ int tspg_pack_noalloc(void *stream, const tspg_csr *M, int major,
                       const uint8_t *mask, void *out_buf, size_t cap,
                       int64_t *nnz_kept_dev);
 
+/* tspg_select_ptrs — the pointer array of a packed tile, in place
+ * (SpaComm::select_ptrs, include/spacomm.cuh:556-623): the counts of the
+ * `len` segments whose mask bit is clear become 0 and ptr[1..len] becomes the
+ * inclusive scan of the counts; the length stays len + 1.  Synchronises
+ * `stream`; TSPG_EOVERFLOW when an int32 offset would pass INT32_MAX. */
+int tspg_select_ptrs(tspg_ctx *ctx, void *stream, void *ptr, int ptr_bits,
+                     int64_t len, const uint8_t *mask);
+
+/* Row offsets <-> row counts, in place on nrows + 1 entries, around the
+ * gather of B tiles (rowptrs_to_rownnz / rownnz_to_rowptrs,
+ * include/utils.cuh:412-448, used at include/tile_holder.cuh:283-327).
+ * tspg_rowptrs_to_rownnz: ptr[i] := ptr[i] - ptr[i-1] for i >= 1 (ptr[0]
+ * kept); stream-ordered.  tspg_rownnz_to_rowptrs: ptr[1..nrows] := its
+ * inclusive scan (ptr[0] kept); synchronises `stream` and returns
+ * TSPG_EOVERFLOW when an int32 offset would pass INT32_MAX. */
+int tspg_rowptrs_to_rownnz(tspg_ctx *ctx, void *stream, void *ptr, int ptr_bits,
+                           int64_t nrows);
+int tspg_rownnz_to_rowptrs(tspg_ctx *ctx, void *stream, void *ptr, int ptr_bits,
+                           int64_t nrows);
+
 /* Size in bytes of a packed tile (CSX_buf_size / compute_message_size,
  * src/hns_spgemm.cu:23-26). */
 size_t tspg_packed_bytes(int64_t nnz, int64_t ptr_len, int val_bits,

@@ -145,3 +145,19 @@ def test_null_context_is_rejected():
     a = TspgCsr()
     assert lib.tspg_spgemm(None, None, C.byref(a), C.byref(a), None, 0) == _lib.TSPG_EINVAL
     assert lib.tspg_ctx_destroy(None) == _lib.TSPG_EINVAL
+
+
+def test_reference_signature_shim_compiles(tmp_path):
+    """include/tspg_trident.hpp exposes the reference's own operator
+    signatures (sp_mma_hybrid, cusparse_spgeam, LocalMatrix::spgemm,
+    SpaCommHandler::Compress, ...): the C++ test that drives them with the
+    reference's call sequence compiles and links against libtspg here (it runs
+    in the GPU suite)."""
+    exe = str(tmp_path / "shim")
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    cmd = ["g++", "-std=c++17", "-O0", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-I", "/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "test_trident_host.cpp"), "-o", exe,
+           "-L", os.path.join(ROOT, "trident_b200"), "-ltspg", "-L", "/usr/local/cuda/lib64", "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]

@@ -120,6 +120,9 @@ def _load() -> C.CDLL:
         "tspg_bitmask_and": (i32, [vp, vp, vp, vp, i64, vp]),
         "tspg_pack": (i32, [vp, vp, P(TspgCsr), i32, vp, vp, sz, vp, P(i64)]),
         "tspg_packed_bytes": (sz, [i64, i64, i32, i32]),
+        "tspg_select_ptrs": (i32, [vp, vp, vp, i32, i64, vp]),
+        "tspg_rowptrs_to_rownnz": (i32, [vp, vp, vp, i32, i64]),
+        "tspg_rownnz_to_rowptrs": (i32, [vp, vp, vp, i32, i64]),
         "tspg_pack_noalloc": (i32, [vp, P(TspgCsr), i32, vp, vp, sz, vp]),
         "tspg_unpack": (i32, [vp, i64, i64, i32, i64, i32, i32, P(TspgCsr)]),
         "tspg_server_create": (i32, [vp, P(TspgServerConfig), P(vp)]),
