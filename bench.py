@@ -16,8 +16,10 @@ the C ABI (flop count, symbolic, scan, numeric) into preallocated C.
   cpu_baseline  the CPU restatement (oracle) on a strided row sample, all host
           threads
 
-Multi-GPU: every rank runs its own replica of the product ("replicas only";
-the plain product has no exchange step), value = sum over ranks.
+Multi-GPU: the rows of A are cut into N panels of equal products; rank 0
+generates A and broadcasts it over NCCL (B = A is replicated), every rank
+multiplies its panel, no reduction ("rowpanels<N>", strong scaling: the
+product is fixed); value = the product's flops / the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -222,48 +224,73 @@ def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
     return float(t.item())
 
 
-def replica_gflops(mults: int, ms: float, world: int) -> float:
-    """Whole-job GFLOP/s of `world` replicas that each did 2 x mults in ms."""
-    return 2.0 * mults / (ms * 1e-3) / 1e9 * world
-
-
 def run_ours(args, rank, world):
+    """One product C = A·A.  At N GPUs the rows of A are cut into N panels of
+    equal products (row-panel split: A is generated on rank 0 and broadcast
+    over NCCL, every rank multiplies its panel by the whole of A, no
+    reduction); at N = 1 the panel is all of A."""
     import ctypes as C
 
     import numpy as np
     import torch
 
-    from trident_b200 import ops
+    from trident_b200 import ops, panels
     from trident_b200._lib import TSPG_F_B_SORTED, TspgCsrOut, check, lib
+    from trident_b200.csr import DeviceCSR
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    A, cfg = make_workload(args)
     ctx = ops.Context(dev)
     cfg_tuning = apply_tuning(ctx, "rmat") if args.workload == "rmat" else None
-    dA = A.to_device(rowptr_bits=32)
+    A = cfg = None
+    if rank == 0:
+        A, cfg = make_workload(args)
+    if world > 1:
+        # B (= A) replicated: one broadcast from rank 0 over NCCL
+        if rank == 0:
+            dA0 = A.to_device(rowptr_bits=32)
+            src = (dA0.rowptr, dA0.col, dA0.val)
+        else:
+            src = (None, None, None)
+        m, n, rp_t, col_t, val_t = panels.broadcast_csr(*src, 0, "cuda", torch.int32, torch.float64,
+                                                        shape=(A.nrows, A.ncols) if rank == 0 else None)
+        dA = DeviceCSR(m, n, rp_t, col_t, val_t)
+        if rank != 0:
+            from trident_b200.synth import HostCSR
+            A = HostCSR(m, n, rp_t.cpu().numpy().astype(np.int64), col_t.cpu().numpy(), val_t.cpu().numpy())
+    else:
+        dA = A.to_device(rowptr_bits=32)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    a = dA.abi()
-    mults, upper = ops.spgemm_count(ctx, dA, dA)
-    plan = ops.Plan(ctx, dA, dA)
+    # the row panel of this rank, cut by products
+    rowf = panels.row_products(ctx, dA, dA).cpu().numpy()
+    mults_total = int(rowf.sum())
+    cuts = panels.panel_cuts(rowf, world)
+    r0, r1 = panels.panel_rows(cuts, rank)
+    a_rp = A.rowptr
+    dP = DeviceCSR(r1 - r0, A.ncols, dA.rowptr[r0:r1 + 1], dA.col, dA.val, nnz=int(a_rp[r1] - a_rp[r0]))
+    pa, b = dP.abi(), dA.abi()
+    mults, upper = ops.spgemm_count(ctx, dP, dA)
+    assert mults == int(rowf[r0:r1].sum())
+    plan = ops.Plan(ctx, dP, dA)
     nnz_c = plan.c_nnz
     plan.close()
+    pm = r1 - r0
     rp_bits = 64 if nnz_c > 2**31 - 1 else 32
-    Crp = torch.empty(A.nrows + 1, dtype=torch.int64 if rp_bits == 64 else torch.int32, device="cuda")
+    Crp = torch.empty(pm + 1, dtype=torch.int64 if rp_bits == 64 else torch.int32, device="cuda")
     Ccol = torch.empty(max(nnz_c, 1), dtype=torch.int32, device="cuda")
     Cval = torch.empty(max(nnz_c, 1), dtype=torch.float64, device="cuda")
 
     def out():
         o = TspgCsrOut()
-        o.nrows, o.ncols = A.nrows, A.ncols
+        o.nrows, o.ncols = pm, A.ncols
         o.rowptr, o.rowptr_bits, o.val_bits = Crp.data_ptr(), rp_bits, 64
         o.col, o.val, o.capacity = Ccol.data_ptr(), Cval.data_ptr(), nnz_c
         return o
 
     def step():
         o = out()
-        check(lib.tspg_spgemm(ctx.h, sp, C.byref(a), C.byref(a), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
+        check(lib.tspg_spgemm(ctx.h, sp, C.byref(pa), C.byref(b), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
 
     for _ in range(args.warmup):
         step()
@@ -294,36 +321,36 @@ def run_ours(args, rank, world):
     launches1 = C.c_int64()
     lib.tspg_ctx_stats(ctx.h, C.byref(launches1))
     ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
-    value = replica_gflops(mults, ms, world)
+    value = 2.0 * mults_total / (ms * 1e-3) / 1e9
 
-    # roofline of the dominant persistent kernel
+    # roofline of the dominant persistent phase of this rank's panel
     bytes_a = csr_bytes(A.nrows, A.nnz, 4)
-    bytes_c = csr_bytes(A.nrows, nnz_c, rp_bits // 8)
-    algo = 2 * bytes_a + bytes_c
+    bytes_p = csr_bytes(pm, int(a_rp[r1] - a_rp[r0]), 4)
+    bytes_c = csr_bytes(pm, nnz_c, rp_bits // 8)
+    algo = bytes_p + bytes_a + bytes_c
     sym, num = statistics.mean(sym_ms), statistics.mean(num_ms)
     dom_ms, dom_name = ((num, "numeric phase (k_phase + k_groups)") if num >= sym
                         else (sym, "symbolic phase (k_phase + k_groups)"))
-    peaks = {}
     try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+        peak, peak_src = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
     except Exception:
         peak, peak_src = 6650.0, "fallback"
     achieved = algo / (dom_ms * 1e-3) / 1e9
-    gather = algo + 8 * A.nnz + 12 * mults
-    traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        ent = prof.get(cfg["workload"], {}).get(dom_name)
-        if ent:
-            traffic = int(ent["dram_bytes_per_launch"])
-    except Exception:
-        pass
+    gather = algo + 8 * int(a_rp[r1] - a_rp[r0]) + 12 * mults
+    traffic = traffic_src = None
+    if world == 1 and rank == 0:
+        try:
+            prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+            ent = prof.get(cfg["workload"], {}).get(dom_name)
+            if ent:
+                traffic, traffic_src = int(ent["dram_bytes_per_launch"]), ent.get("source")
+        except Exception:
+            pass
 
     # e2e through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, (Crp, Ccol, Cval))
+        e2e = run_e2e(args, A, ctx, mults_total, nnz_c, rp_bits, world, (Crp, Ccol, Cval), (r0, r1))
 
     cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -335,35 +362,39 @@ def run_ours(args, rank, world):
         parity = parity_rows(A, A, rows, Crp, Ccol, Cval)
         parity["sample"] = cpu["sample"]
 
-    line = {
-        "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64",
-        "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
-        "config": dict(cfg, mults=mults),
-        "parallelism": f"replicas{world}",
-        "output": {"nnz_C": nnz_c, "c_rowptr_bits": rp_bits, "C_MB": round(bytes_c / 1e6)},
-        "tuning": cfg_tuning,
-        "phase_ms": {"symbolic": round(sym, 3), "numeric": round(num, 3)},
-        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
-                     "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": traffic, "algorithmic_bytes": algo,
-                     "step_frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4),
-                     # Gustavson gather model: + B row offsets per A entry + B row contents per product
-                     "gather_model_bytes": gather,
-                     "gather_frac": round(gather / (dom_ms * 1e-3) / 1e9 / peak, 4)},
-        "gpu_launches": int(launches1.value - launches0.value),
-        "clocks": clk,
-        "e2e": e2e,
-        "cpu_baseline": cpu,
-        "parity": parity,
-    }
+    line = None
+    if rank == 0:
+        line = {
+            "metric": "A·A SpGEMM GFLOP/s (2 x multiply-adds), FP64",
+            "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded R-MAT, values U[-1,1])",
+            "config": dict(cfg, mults=mults_total),
+            "parallelism": f"rowpanels{world}" if world > 1 else "single",
+            "panels": {"cuts": [int(x) for x in cuts], "rank0_mults": mults} if world > 1 else None,
+            "output": {"nnz_C": nnz_c, "c_rowptr_bits": rp_bits, "C_MB": round(bytes_c / 1e6)},
+            "tuning": cfg_tuning,
+            "phase_ms": {"symbolic": round(sym, 3), "numeric": round(num, 3)},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "traffic_source": traffic_src, "algorithmic_bytes": algo,
+                         "step_frac": round(algo / (ms * 1e-3) / 1e9 / peak, 4),
+                         # Gustavson gather model: + B row offsets per A entry + B row contents per product
+                         "gather_model_bytes": gather,
+                         "gather_frac": round(gather / (dom_ms * 1e-3) / 1e9 / peak, 4)},
+            "gpu_launches": int(launches1.value - launches0.value),
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "parity": parity,
+        }
     ctx.close()
     return line
 
 
-def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
-    """Host A (pinned) -> device, SpGEMM through the ABI, C -> pinned host."""
+def run_e2e(args, A, ctx, mults_total, nnz_c, rp_bits, world, cbufs, panel):
+    """Host A (pinned) -> device, this rank's panel of A·A through the ABI,
+    the panel of C -> pinned host."""
     import ctypes as C
 
     import numpy as np
@@ -371,6 +402,8 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
 
     from trident_b200._lib import TSPG_F_B_SORTED, TspgCsr, TspgCsrOut, check, lib
 
+    r0, r1 = panel
+    pm = r1 - r0
     hrp = torch.from_numpy(A.rowptr.astype(np.int32)).pin_memory()
     hcol = torch.from_numpy(A.col).pin_memory()
     hval = torch.from_numpy(A.val).pin_memory()
@@ -378,12 +411,12 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
         torch.empty_like(hval, device="cuda")
     # C lands in pinned host memory; when that does not fit, it is streamed
     # through a pinned staging ring (every byte still crosses to the host)
-    c_bytes = nnz_c * 12 + (A.nrows + 1) * (rp_bits // 8)
+    c_bytes = nnz_c * 12 + (pm + 1) * (rp_bits // 8)
     try:
         avail = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_AVPHYS_PAGES")
     except Exception:
         avail = 0
-    full = c_bytes < 0.5 * avail
+    full = c_bytes * world < 0.5 * avail
     rdt = torch.int64 if rp_bits == 64 else torch.int32
     Crp, Ccol, Cval = cbufs
     if full:
@@ -395,6 +428,7 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
         hC = torch.empty(ring, dtype=torch.uint8, pin_memory=True)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
+    pnnz = int(A.rowptr[r1] - A.rowptr[r0])
 
     def d2h_ring(t):
         flat = t.view(torch.uint8)
@@ -406,12 +440,13 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
         drp.copy_(hrp, non_blocking=True)
         dcol.copy_(hcol, non_blocking=True)
         dval.copy_(hval, non_blocking=True)
-        a = TspgCsr(A.nrows, A.ncols, A.nnz, drp.data_ptr(), 32, 64, dcol.data_ptr(), dval.data_ptr())
+        b = TspgCsr(A.nrows, A.ncols, A.nnz, drp.data_ptr(), 32, 64, dcol.data_ptr(), dval.data_ptr())
+        a = TspgCsr(pm, A.ncols, pnnz, drp.data_ptr() + 4 * r0, 32, 64, dcol.data_ptr(), dval.data_ptr())
         o = TspgCsrOut()
-        o.nrows, o.ncols = A.nrows, A.ncols
+        o.nrows, o.ncols = pm, A.ncols
         o.rowptr, o.rowptr_bits, o.val_bits = Crp.data_ptr(), rp_bits, 64
         o.col, o.val, o.capacity = Ccol.data_ptr(), Cval.data_ptr(), nnz_c
-        check(lib.tspg_spgemm(ctx.h, sp, C.byref(a), C.byref(a), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
+        check(lib.tspg_spgemm(ctx.h, sp, C.byref(a), C.byref(b), C.byref(o), TSPG_F_B_SORTED), "tspg_spgemm")
         if full:
             hC[0].copy_(Crp, non_blocking=True)
             hC[1].copy_(Ccol[:nnz_c], non_blocking=True)
@@ -424,6 +459,8 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
     steps = max(1, min(args.steps, 3))
     step()
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(steps):
@@ -432,8 +469,15 @@ def run_e2e(args, A, ctx, mults, nnz_c, rp_bits, world, cbufs):
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1) / steps, world)
     h2d = (hrp.numel() * 4 + hcol.numel() * 4 + hval.numel() * 8)
-    return {"value": round(replica_gflops(mults, ms, world), 3), "unit": "GFLOP/s",
-            "ms_per_step": round(ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(c_bytes),
+    d2h = c_bytes
+    if world > 1:
+        t = torch.tensor([c_bytes], dtype=torch.int64, device="cuda")
+        torch.distributed.all_reduce(t)
+        d2h = int(t.item())
+    return {"value": round(2.0 * mults_total / (ms * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+            "ms_per_step": round(ms, 3), "h2d_bytes_per_step": int(h2d * world), "d2h_bytes_per_step": int(d2h),
+            "per": "whole job: every rank copies all of A (its panel and the replicated B) and its panel of C"
+            if world > 1 else "A to the device, C to the host",
             "c_to_host": "pinned result arrays" if full else "pinned 1 GiB staging ring (host RAM < 2x C)",
             "steps": steps}
 

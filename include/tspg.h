@@ -192,9 +192,20 @@ int tspg_spgemm_count_mask(tspg_ctx *ctx, void *stream, const tspg_csr *A,
                            const tspg_csr *B, uint8_t *mask, int64_t *mults,
                            int64_t *c_nnz_upper);
 
+/* tspg_spgemm_row_products — products per row of A·B into the device int64
+ * array out[nrows(A)]: out[i] = sum over A's entries (i, k) of nnz(B row k).
+ * Stream-ordered.  Its prefix sum cuts A's rows into panels of equal work for
+ * the row-panel split of one product over several GPUs (no reference
+ * counterpart: the reference splits by tiles, src/hns_spgemm.cu). */
+int tspg_spgemm_row_products(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                             const tspg_csr *B, int64_t *out);
+
 /* tspg_spgemm — C = A·B, two-phase inside (symbolic, then numeric).
  * Replaces LocalMatrix::spgemm (include/KokkosWrap.hpp:367-391) and
  * cusparse_spgemm / _reuse / _mem (include/cusparse_helpers.cuh:908-1344).
+ * A's row offsets need not start at 0: a view of rows [r0, r1) of a larger
+ * CSR (rowptr advanced by r0, col and val unchanged) is a valid A, which is
+ * how a row panel of one product is computed on its own GPU.
  * Empty operands give an empty C with a zeroed rowptr (the num_prods == 0
  * exit, include/cusparse_helpers.cuh:1251-1257).  Synchronises `stream` once
  * (to learn nnz(C)). */

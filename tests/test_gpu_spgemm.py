@@ -214,3 +214,26 @@ def test_uniform_rows_expand_sort_compress(ctx, lam):
                             M.val.astype(np.float32).astype(np.float64))
     C32 = ops.spgemm(ctx, A.to_device(val_bits=32), B.to_device(val_bits=32))
     check_product(C32, r32(A), r32(B), tol=TOL32)
+
+
+def test_row_panels_concatenate_to_the_product(ctx):
+    """The row-panel split of the multi-GPU benchmark on one GPU: A's rows cut
+    by equal products (tspg_spgemm_row_products), each panel multiplied as a
+    view whose row offsets do not start at 0; the panels concatenate to the
+    oracle's product."""
+    from trident_b200 import panels
+    from trident_b200.csr import DeviceCSR
+    A = workloads.rmat(scale=12, edge_factor=16, seed=7)
+    dA = A.to_device()
+    rowf = panels.row_products(ctx, dA, dA).cpu().numpy()
+    np.testing.assert_array_equal(rowf, oracle.row_mults(A, A))
+    cuts = panels.panel_cuts(rowf, 3)
+    parts = []
+    for r in range(3):
+        r0, r1 = panels.panel_rows(cuts, r)
+        dP = DeviceCSR(r1 - r0, A.ncols, dA.rowptr[r0:r1 + 1], dA.col, dA.val,
+                       nnz=int(A.rowptr[r1] - A.rowptr[r0]))
+        H = ops.spgemm(ctx, dP, dA).to_host()
+        parts.append((H.rowptr, H.col, H.val))
+    rp, cj, cx = panels.assemble(parts, A.ncols)
+    check_product(HostCSR(A.nrows, A.ncols, rp, cj, cx), A, A)

@@ -104,6 +104,7 @@ def _load() -> C.CDLL:
         "tspg_batch_count": (i32, [vp, vp, P(i64), P(i64)]),
         "tspg_batch_result": (i32, [vp, i32, P(TspgCsr)]),
         "tspg_spgemm_count": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(i64), P(i64)]),
+        "tspg_spgemm_row_products": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), vp]),
         "tspg_spgemm_count_mask": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), vp, P(i64), P(i64)]),
         "tspg_spgemm": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), P(TspgCsrOut), i32]),
         "tspg_spgemm_symbolic": (i32, [vp, vp, P(TspgCsr), P(TspgCsr), i32, P(vp), P(i64)]),

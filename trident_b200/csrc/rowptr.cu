@@ -3,6 +3,8 @@
 // rowptrs_to_rownnz / rownnz_to_rowptrs, include/utils.cuh:412-448, used at
 // include/tile_holder.cuh:283-327), and the masked pointer pack of a tile
 // (select_ptrs, include/spacomm.cuh:556-623) built from them.
+#include <algorithm>
+
 #include "spgemm_kernels.cuh"
 
 namespace tspg {
@@ -116,6 +118,35 @@ int select_ptrs_impl(tspg_ctx *ctx, cudaStream_t s, PT *ptr, int64_t len, const 
   return to_rowptrs<PT>(ctx, s, ptr, len);
 }
 
+// products of row r of A·B: sum over A's entries (r, k) of nnz(B row k); one
+// warp per row
+template <typename PA, typename PB>
+__global__ void __launch_bounds__(256)
+    k_row_products(const PA *Ap, const int32_t *Aj, const PB *Bp, int64_t m, int64_t *out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < m; r += nw) {
+    int64_t f = 0;
+    for (int64_t q = int64_t(Ap[r]) + lane; q < int64_t(Ap[r + 1]); q += 32) {
+      const int32_t k = Aj[q];
+      f += int64_t(Bp[k + 1]) - int64_t(Bp[k]);
+    }
+    f = warp_sum(f);
+    if (lane == 0) out[r] = f;
+  }
+}
+
+template <typename PA, typename PB>
+int row_products_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A, const tspg_csr *B, int64_t *out) {
+  if (A->nrows == 0) return TSPG_OK;
+  const int64_t blocks = std::min<int64_t>((A->nrows * 32 + 255) / 256, int64_t(ctx->num_sms) * 16);
+  k_row_products<PA, PB><<<(unsigned)blocks, 256, 0, s>>>((const PA *)A->rowptr, A->col, (const PB *)B->rowptr,
+                                                         A->nrows, out);
+  ctx->launches += 1;
+  TSPG_CUDA(ctx, cudaGetLastError());
+  return TSPG_OK;
+}
+
 int check_ptr_args(tspg_ctx *ctx, void *ptr, int ptr_bits, int64_t n) {
   if (!ctx || !ptr || n < 0) return TSPG_EINVAL;
   if (ptr_bits != 32 && ptr_bits != 64) return TSPG_EINVAL;
@@ -153,4 +184,20 @@ extern "C" int tspg_select_ptrs(tspg_ctx *ctx, void *stream, void *ptr, int ptr_
   cudaStream_t s = (cudaStream_t)stream;
   return ptr_bits == 32 ? select_ptrs_impl<int32_t>(ctx, s, (int32_t *)ptr, len, mask)
                         : select_ptrs_impl<int64_t>(ctx, s, (int64_t *)ptr, len, mask);
+}
+
+extern "C" int tspg_spgemm_row_products(tspg_ctx *ctx, void *stream, const tspg_csr *A,
+                                        const tspg_csr *B, int64_t *out) {
+  if (!ctx || !out) return TSPG_EINVAL;
+  TSPG_TRY(check_csr(A));
+  TSPG_TRY(check_csr(B));
+  if (A->ncols != B->nrows) return TSPG_EINVAL;
+  if (A->nnz > 0 && B->nrows > 0 && !B->rowptr) return TSPG_EINVAL;
+  TSPG_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (A->rowptr_bits == 32)
+    return B->rowptr_bits == 32 ? row_products_impl<int32_t, int32_t>(ctx, s, A, B, out)
+                                : row_products_impl<int32_t, int64_t>(ctx, s, A, B, out);
+  return B->rowptr_bits == 32 ? row_products_impl<int64_t, int32_t>(ctx, s, A, B, out)
+                              : row_products_impl<int64_t, int64_t>(ctx, s, A, B, out);
 }
