@@ -148,6 +148,22 @@ def pack(ptr, idx, val, mask):
     return optr, oidx[:kept], oval[:kept]
 
 
+def transpose(M):
+    """T = M^T as CSR with sorted rows: the CSR of a CSC tile, the job of
+    cusparse_csc_to_csr (include/cusparse_helpers.cuh:607-705) and
+    LocalMatrix::csc_to_csr (include/KokkosWrap.hpp:442-531).  Restated as a
+    stable counting sort of M's entries by column: row j of T lists the
+    entries of column j of M in M's row order (repeated entries kept).
+    Returns (rowptr int64 of M.ncols + 1, col int32, val)."""
+    rp = np.asarray(M.rowptr, dtype=np.int64)
+    col = np.asarray(M.col, dtype=np.int64)
+    rows = np.repeat(np.arange(M.nrows, dtype=np.int64), np.diff(rp))
+    order = np.argsort(col, kind="stable")
+    trp = np.zeros(M.ncols + 1, dtype=np.int64)
+    np.cumsum(np.bincount(col, minlength=M.ncols), out=trp[1:])
+    return trp, rows[order].astype(np.int32), np.asarray(M.val)[order]
+
+
 def coo_to_csx(nmaj: int, maj, mnr, val):
     """COO -> compressed by `maj`: the host builders coo_to_row_csx /
     coo_to_col_csx (include/cusparse_helpers.cuh:17-131) and coo_to_kokkos_crs

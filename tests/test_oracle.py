@@ -225,3 +225,19 @@ def test_summa_tiles_cover_the_matrix():
     np.testing.assert_array_equal(M.indptr, A.rowptr)
     np.testing.assert_array_equal(M.indices, A.col)
     np.testing.assert_array_equal(M.data, A.val)
+
+
+def test_transpose_vs_scipy_and_host_generator():
+    """The oracle's transpose (the checker of the device transpose) equals
+    scipy's and keeps entries of a column in row order."""
+    from helpers import random_csr
+    M = random_csr(300, 200, density=0.03, seed=9)
+    rp, col, val = oracle.transpose(M)
+    T = M.to_scipy().T.tocsr()
+    T.sort_indices()
+    np.testing.assert_array_equal(rp, T.indptr)
+    np.testing.assert_array_equal(col, T.indices)
+    np.testing.assert_array_equal(val, T.data)
+    R = workloads.transpose(M)
+    np.testing.assert_array_equal(R.rowptr, rp)
+    np.testing.assert_array_equal(R.col, col)
