@@ -237,3 +237,80 @@ def test_row_panels_concatenate_to_the_product(ctx):
         parts.append((H.rowptr, H.col, H.val))
     rp, cj, cx = panels.assemble(parts, A.ncols)
     check_product(HostCSR(A.nrows, A.ncols, rp, cj, cx), A, A)
+
+
+def _window_operands(val_dtype=np.float64):
+    """Operands whose heavy rows take the column-window DENSE form (with the
+    window threshold at 2^10 products): B has 40000 columns (windows of 16384:
+    two full, one partial), 20 hub rows of 12000 sorted columns (segments
+    longer than one thread's 8 loads: the warp pass), 4000 short rows, and
+    5000 rows of 12 columns inside the first window (one A row takes all of
+    them: more long segments than the queue holds); one A row has 9020 entries
+    (cursors in global memory); in the last A row one pair of products
+    cancels exactly and one product is -0.0 (both stay in the pattern)."""
+    rng = np.random.default_rng(21)
+    n = 40000
+    rows = [np.sort(rng.choice(n, 12000, replace=False)) for _ in range(20)]
+    rows += [np.sort(rng.choice(n, 10, replace=False)) for _ in range(4000)]
+    rows += [np.sort(rng.choice(16384, 12, replace=False)) for _ in range(5000)]
+    p0 = len(rows)
+    rows += [np.array([7, 20000, 39999]), np.array([7, 39998])]
+    brp = np.zeros(len(rows) + 1, np.int64)
+    brp[1:] = np.cumsum([r.size for r in rows])
+    bcol = np.concatenate(rows).astype(np.int32)
+    bval = rng.uniform(-1, 1, bcol.size)
+    bval[brp[p0]] = 0.5       # B[p0, 7]
+    bval[brp[p0] + 1] = 0.0   # B[p0, 20000]
+    bval[brp[p0 + 1]] = 0.5   # B[p0 + 1, 7]
+    B = HostCSR(len(rows), n, brp, bcol, bval.astype(val_dtype).astype(np.float64))
+    arows = [np.sort(np.concatenate([rng.choice(20, 3, replace=False), 20 + rng.choice(4000, 300, replace=False)]))
+             for _ in range(12)]                    # hubs + short rows
+    arows.append(np.arange(4020, 9020))             # 5000 long segments in window 0
+    arows.append(np.arange(0, 9020))                # 9020 entries: cursors in global memory
+    hub = next(h for h in range(20) if 7 not in rows[h] and 20000 not in rows[h])
+    arows.append(np.array([hub, p0, p0 + 1]))      # -1 * 0.5 + 1 * 0.5 = 0 at column 7; -1 * 0.0 = -0.0
+    arp = np.zeros(len(arows) + 1, np.int64)
+    arp[1:] = np.cumsum([r.size for r in arows])
+    acol = np.concatenate(arows).astype(np.int32)
+    aval = rng.uniform(-1, 1, acol.size)
+    aval[arp[-2] + 1], aval[arp[-2] + 2] = -1.0, 1.0
+    A = HostCSR(len(arows), B.nrows, arp, acol, aval.astype(val_dtype).astype(np.float64))
+    return A, B
+
+
+@pytest.mark.parametrize("win", [10, 0])
+def test_dense_window_form(win):
+    """The column-window form (win = 10) and the rank form (win = 0) on the
+    same heavy rows: both equal the oracle (structure bit-exact, values within
+    1e-12), including the exact cancellation and the -0.0 product."""
+    c = ops.Context(0)
+    c.set_tuning({"dense_win_log2": win, "num_lim": [1, 1, 1, 1], "sym_lim": [1, 1, 1, 1]})
+    A, B = _window_operands()
+    H = check_product(ops.spgemm(c, A.to_device(), B.to_device(), flags=TSPG_F_B_SORTED), A, B)
+    r = A.nrows - 1
+    row = H.col[H.rowptr[r]:H.rowptr[r + 1]]
+    assert 7 in row and H.val[H.rowptr[r] + int(np.searchsorted(row, 7))] == 0.0
+    assert 20000 in row
+    torch.cuda.synchronize()
+    c.close()
+
+
+def test_dense_window_form_fp32_and_addend():
+    """FP32 twin, and the fused accumulate (the addend's entries join every
+    window)."""
+    from trident_b200._lib import TSPG_F_ACC_FUSE
+    c = ops.Context(0)
+    c.set_tuning({"dense_win_log2": 10, "num_lim": [1, 1, 1, 1], "sym_lim": [1, 1, 1, 1]})
+    A, B = _window_operands(np.float32)
+    C32 = ops.spgemm(c, A.to_device(val_bits=32), B.to_device(val_bits=32), flags=TSPG_F_B_SORTED)
+    check_product(C32, A, B, tol=TOL32)
+    E = random_csr(A.nrows, B.ncols, per_row=3000, seed=31)
+    D = ops.sp_mma(c, A.to_device(), B.to_device(), E.to_device(), flags=TSPG_F_ACC_FUSE)
+    rp, cj, cx, ca = oracle.spgemm(A, B)
+    S = oracle.spadd(HostCSR(A.nrows, B.ncols, rp, cj, cx), E)
+    H = D.to_host()
+    np.testing.assert_array_equal(H.rowptr, S[0])
+    np.testing.assert_array_equal(H.col, S[1])
+    assert np.all(np.abs(H.val - S[2]) <= 1e-12 * np.maximum(1.0, np.abs(S[2])) * 8)
+    torch.cuda.synchronize()
+    c.close()

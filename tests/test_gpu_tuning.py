@@ -9,9 +9,9 @@ from trident_b200._lib import TSPG_EINVAL, TspgError
 pytestmark = pytest.mark.gpu
 
 TUNINGS = [
-    {"sym_lim": [128, 1024, 2048, 8192], "num_lim": [128, 512, 1024, 4096], "hash_load": 4},
-    {"sym_lim": [512, 512, 512, 512], "num_lim": [256, 256, 256, 256], "hash_load": 2},
-    {"sym_lim": [1, 1, 1, 1], "num_lim": [1, 1, 1, 1], "hash_load": 8},
+    {"sym_lim": [128, 1024, 2048, 8192], "num_lim": [128, 512, 1024, 4096], "hash_load": 4, "dense_win_log2": 17},
+    {"sym_lim": [512, 512, 512, 512], "num_lim": [256, 256, 256, 256], "hash_load": 2, "dense_win_log2": 0},
+    {"sym_lim": [1, 1, 1, 1], "num_lim": [1, 1, 1, 1], "hash_load": 8, "dense_win_log2": 10},
 ]
 
 
@@ -24,7 +24,7 @@ def tctx():
 
 def test_invalid_tuning_refused(tctx):
     for bad in ({"num_lim": [1024, 1024, 2048, 8192]}, {"sym_lim": [512, 256, 4096, 24576]},
-                {"hash_load": 3}, {"num_lim": [0, 1024, 2048, 8192]}):
+                {"hash_load": 3}, {"num_lim": [0, 1024, 2048, 8192]}, {"dense_win_log2": 9}):
         with pytest.raises(TspgError) as e:
             tctx.set_tuning(bad)
         assert e.value.status == TSPG_EINVAL

@@ -20,6 +20,7 @@ def test_neighbours_are_valid_and_differ_in_one_slot():
         diff = sum(a != b for a, b in zip(u["sym_lim"], t["sym_lim"]))
         diff += sum(a != b for a, b in zip(u["num_lim"], t["num_lim"]))
         diff += u["hash_load"] != t["hash_load"]
+        diff += u["dense_win_log2"] != t["dense_win_log2"]
         assert diff == 1
         seen += 1
     assert seen > 10
@@ -33,6 +34,8 @@ def test_validity_rule():
     assert not tune.valid(bad)
     bad = dict(t, hash_load=3)
     assert not tune.valid(bad)
+    assert not tune.valid(dict(t, dense_win_log2=5))
+    assert tune.valid(dict(t, dense_win_log2=0))
 
 
 def test_committed_tuning_files_are_valid():

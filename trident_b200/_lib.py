@@ -57,7 +57,8 @@ class TspgTuning(C.Structure):
         ("sym_lim", C.c_int32 * 4),
         ("num_lim", C.c_int32 * 4),
         ("hash_load", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("dense_win_log2", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

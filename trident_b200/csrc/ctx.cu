@@ -182,6 +182,7 @@ extern "C" int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t) {
     u.num[i] = t->num_lim[i];
   }
   u.load = t->hash_load;
+  u.win = t->dense_win_log2;
   if (!tune_valid(u)) return TSPG_EINVAL;
   ctx->tune = u;
   return TSPG_OK;
@@ -194,7 +195,8 @@ extern "C" int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t) {
     t->num_lim[i] = ctx->tune.num[i];
   }
   t->hash_load = ctx->tune.load;
-  t->reserved[0] = t->reserved[1] = t->reserved[2] = 0;
+  t->dense_win_log2 = ctx->tune.win;
+  t->reserved[0] = t->reserved[1] = 0;
   return TSPG_OK;
 }
 

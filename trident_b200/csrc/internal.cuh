@@ -28,8 +28,10 @@ struct Tune {
   int32_t sym[4];
   int32_t num[4];
   int32_t load;
-  int32_t pad[3];
+  int32_t win;  // log2 of the products from which DENSE numeric rows take the window form; 0 = never
+  int32_t pad[2];
 };
+constexpr int32_t kDefaultWinLog2 = 17;
 
 // A tuning is valid when every bound is positive, non-decreasing over the
 // classes and within the table capacity of its class, and load is 2, 4 or 8.
@@ -40,6 +42,7 @@ inline bool tune_valid(const Tune &t) {
     if (t.sym[i] < 1 || t.sym[i] > smax[i] || t.num[i] < 1 || t.num[i] > nmax[i]) return false;
     if (i > 0 && (t.sym[i] < t.sym[i - 1] || t.num[i] < t.num[i - 1])) return false;
   }
+  if (t.win != 0 && (t.win < 10 || t.win > 40)) return false;
   return t.load == 2 || t.load == 4 || t.load == 8;
 }
 }  // namespace tspg
@@ -72,7 +75,8 @@ struct tspg_ctx {
                      {int32_t(tspg::kNumLim32), int32_t(tspg::kNumLim128),
                       int32_t(tspg::kNumLim256), int32_t(tspg::kNumLim1024)},
                      2,
-                     {0, 0, 0}};
+                     tspg::kDefaultWinLog2,
+                     {0, 0}};
 };
 
 namespace tspg {

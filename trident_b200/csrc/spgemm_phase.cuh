@@ -1219,6 +1219,217 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   }
 }
 
+// DENSE numeric row, column-window form, for heavy rows with sorted B whose
+// output fills at least 1/16 of the columns.  The row's columns are swept in
+// windows of kWinCols; a window accumulates in a shared FP64 array indexed by
+// column — one shared atomic per product, and no bitmap: a slot that still
+// holds the bit pattern of -0.0 is empty, because every product is added as
+// a*b + 0.0 (never -0.0 under round-to-nearest) and an IEEE sum is -0.0 only
+// when all its terms are — then compacted in column order and written to C
+// once, coalesced.  No global reductions, no zero fill of C, one pass over
+// the products.  Every A entry keeps a cursor into its B row and the column
+// at the cursor (an entry with nothing in the window costs one load).
+// Pass 1: thread t takes entries t, t + 512, ... and walks U B entries from
+// the cursor; an entry whose window segment goes on is queued, and pass 2
+// walks each queued segment with a whole warp (U x 32 entries per step), so a
+// hub row of B never holds up a warp of short entries (with one thread per
+// whole segment, R-MAT rows kept 5 of 32 lanes busy).  Compaction: warp w owns
+// 1/16 of the window, takes 32 slots per step, keeps the step ballots in
+// registers (lane s holds step s), and a scan of the 16 warp counts places its
+// entries.
+constexpr int kWinCols = 16384;   // columns per window (128 KiB of FP64)
+constexpr int kWinQueue = 4096;   // queued long segments per window
+static_assert(kWinCols * 8 + 2 * kDenseCurSmem * 4 + kWinQueue * 4 <= kDynSmem, "window smem");
+
+template <typename PT, typename VT>
+__device__ void num_dense_win_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
+                                  int64_t idx, unsigned char *smem, const GroupMem &gm) {
+  using UT = std::conditional_t<sizeof(VT) == 8, unsigned long long, unsigned>;
+  constexpr UT kEmpty = UT(1) << (sizeof(VT) * 8 - 1);  // -0.0
+  constexpr int U = 8;
+  constexpr int NWARP = kThreads / 32;
+  constexpr int PER = kWinCols / NWARP;  // slots per warp
+  constexpr int STEPS = PER / 32;
+  static_assert(STEPS == 32, "one ballot per lane");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  VT *acc = (VT *)smem;
+  UT *accb = (UT *)smem;
+  int32_t *cur_s = (int32_t *)(smem + kWinCols * sizeof(VT));
+  int32_t *nxc_s = cur_s + kDenseCurSmem;
+  int32_t *queue = nxc_s + kDenseCurSmem;
+  const RowRef rr = decode_row(A, idx);
+  const ProdDev<PT, VT> &P = prods[rr.p];
+  const int64_t n = P.n;
+  const int64_t a0 = P.Ap[rr.r], a1 = P.Ap[rr.r + 1], na = a1 - a0;
+  const int64_t c = A.rowc[rr.g];
+  int32_t *cur = na <= kDenseCurSmem ? cur_s : A.curbuf + 2 * blockIdx.x * A.cur_stride;
+  int32_t *nxc = na <= kDenseCurSmem ? nxc_s : cur + A.cur_stride;
+  const int32_t *__restrict__ Aj = P.Aj;
+  const VT *__restrict__ Ax = P.Ax;
+  const PT *__restrict__ Bp = P.Bp;
+  const int32_t *__restrict__ Bj = P.Bj;
+  const VT *__restrict__ Bx = P.Bx;
+  int *nq = gm.nl;
+  long long tp = clock64();
+  for (int i = tid; i < kWinCols; i += kThreads) accb[i] = kEmpty;
+  for (int64_t j = tid; j < na; j += kThreads) {
+    const int64_t k = __ldg(Aj + a0 + j);
+    const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+    cur[j] = 0;
+    nxc[j] = b1 > b0 ? __ldg(Bj + b0) : INT32_MAX;
+  }
+  if (tid == 0) *nq = 0;
+  __syncthreads();
+  prof_sub(A, 5, tp);
+  const uint64_t pass = policy_evict_first();
+  int64_t out = A.cp[rr.g] - A.cp[A.base[rr.p]];
+  int64_t emitted = 0;
+  int32_t *__restrict__ Cj = P.Cj;
+  VT *__restrict__ Cx = P.Cx;
+  for (int64_t w0 = 0; w0 < n; w0 += kWinCols) {
+    const int64_t w1 = (w0 + kWinCols < n) ? w0 + kWinCols : n;
+    const int32_t w0i = int32_t(w0);  // columns are int32 (n <= INT32_MAX)
+    const unsigned wlen = unsigned(w1 - w0);
+    // pass 1: one thread per entry, U B entries from the cursor
+    for (int64_t j = tid; j < na; j += kThreads) {
+      if (nxc[j] >= w1) continue;  // nothing in this window
+      const int64_t k = __ldg(Aj + a0 + j);
+      const VT a = __ldg(Ax + a0 + j);
+      const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+      int64_t q = b0 + cur[j];
+      bool tried = false, queued = false;
+      int32_t nextc = INT32_MAX;
+      while (true) {
+        int32_t cc[U];
+        VT xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t qq = q + u;
+          cc[u] = qq < b1 ? __ldg(Bj + qq) : INT32_MAX;
+          xv[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
+        }
+        int nin = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          // in the window (one unsigned compare: a column below w0 — only
+          // possible when B's rows are not sorted as promised — is skipped,
+          // never written out of bounds)
+          if (unsigned(cc[u] - w0i) < wlen) {
+            atomicAdd(acc + (cc[u] - w0i), a * xv[u] + VT(0));
+            ++nin;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (u == nin) nextc = cc[u];  // the first column past the window (sorted B)
+        q += nin;
+        if (nin < U) break;
+        if (q >= b1) {
+          nextc = INT32_MAX;
+          break;
+        }
+        if (!tried) {  // the segment goes on: hand it to a warp
+          tried = true;
+          const int slot = atomicAdd(nq, 1);
+          if (slot < kWinQueue) {
+            queue[slot] = int32_t(j);
+            queued = true;
+            break;
+          }
+        }
+      }
+      cur[j] = int32_t(q - b0);
+      if (!queued) nxc[j] = nextc;
+    }
+    // the addend row of the accumulate form: every window takes its columns
+    for_addend<true>(P, rr.r, tid, kThreads, [&](int32_t col, VT v) {
+      if (col >= w0 && col < w1) atomicAdd(acc + (col - w0i), v + VT(0));
+    });
+    __syncthreads();
+    prof_sub(A, 6, tp);
+    // pass 2: a warp per queued segment, U x 32 B entries per step
+    const int nqueued = min(*nq, kWinQueue);
+    for (int i = warp; i < nqueued; i += NWARP) {
+      const int64_t j = queue[i];
+      const int64_t k = __ldg(Aj + a0 + j);
+      const VT a = __ldg(Ax + a0 + j);
+      const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
+      int64_t q = b0 + cur[j];
+      while (q < b1) {
+        int32_t cc[U];
+        VT xv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t qq = q + u * 32 + lane;
+          cc[u] = qq < b1 ? __ldg(Bj + qq) : INT32_MAX;
+          xv[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
+        }
+        int nin = 0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          // in the window (one unsigned compare: a column below w0 — only
+          // possible when B's rows are not sorted as promised — is skipped,
+          // never written out of bounds)
+          if (unsigned(cc[u] - w0i) < wlen) {
+            atomicAdd(acc + (cc[u] - w0i), a * xv[u] + VT(0));
+            ++nin;
+          }
+        }
+        nin = __reduce_add_sync(0xffffffffu, nin);
+        q += nin;  // sorted B: the entries below w1 are a prefix of the segment
+        if (nin < U * 32) break;
+      }
+      if (lane == 0) {
+        cur[j] = int32_t(q - b0);
+        nxc[j] = q < b1 ? __ldg(Bj + q) : INT32_MAX;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) *nq = 0;
+    prof_sub(A, 7, tp);
+    // compaction: ballots of the warp's 32 steps, one per lane
+    unsigned mine = 0;
+    int wcount = 0;
+    const int sbase = warp * PER;
+#pragma unroll 4
+    for (int st = 0; st < STEPS; ++st) {
+      const unsigned b = __ballot_sync(0xffffffffu, accb[sbase + st * 32 + lane] != kEmpty);
+      if (lane == st) mine = b;
+      wcount += __popc(b);
+    }
+    if (lane == 0) gm.tmp[warp] = wcount;
+    __syncthreads();
+    int64_t wbase = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < NWARP; ++w) {
+      const int64_t v = gm.tmp[w];
+      if (w < warp) wbase += v;
+      total += v;
+    }
+    int64_t pos = out + wbase;
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll 4
+    for (int st = 0; st < STEPS; ++st) {
+      const unsigned b = __shfl_sync(0xffffffffu, mine, st);
+      if ((b >> lane) & 1u) {
+        const int s = sbase + st * 32 + lane;
+        const int64_t e = pos + __popc(b & lt);
+        if (emitted + (e - out) < c) {  // e < the row's end unless the counts broke
+          store_hint(Cj + e, int32_t(w0 + s), pass);
+          store_hint(Cx + e, acc[s], pass);
+        }
+        accb[s] = kEmpty;
+      }
+      pos += __popc(b);
+    }
+    out += total;
+    emitted += total;
+    __syncthreads();  // the slots are empty again and gm.tmp is free
+    prof_sub(A, 8, tp);
+  }
+  if (tid == 0 && emitted != c) set_error(A.err, 109);
+}
+
 // ---------------------------------------------------------------- the kernel
 
 struct PhaseShared {
@@ -1386,8 +1597,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     const long long t0 = clock64();
     if (cls_dense(c)) {
       if constexpr (NUM) {
-        const ProdDev<PT, VT> &P = prods[decode_row(A, idx).p];
-        if (P.n <= kRankMaxCols)
+        const RowRef rr = decode_row(A, idx);
+        const ProdDev<PT, VT> &P = prods[rr.p];
+        // heavy rows whose output fills >= 1/16 of the columns: column windows
+        const int win = A.S->tune.win;
+        if (P.b_sorted && win > 0 && A.rowf[rr.g] >= (int64_t(1) << win) &&
+            int64_t(A.rowc[rr.g]) * 16 >= P.n)
+          num_dense_win_row<PT, VT>(prods, A, idx, smem, gm);
+        else if (P.n <= kRankMaxCols)
           num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm);
         else
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);

@@ -32,12 +32,16 @@ NUM_CAP = [256, 1024, 2048, 8192]
 SYM_CHOICES = [[128, 256, 512], [1024, 2048], [2048, 3072, 4096], [8192, 12288, 24576]]
 NUM_CHOICES = [[128, 192, 256], [512, 768, 1024], [1024, 1536, 2048], [4096, 6144, 8192]]
 LOAD_CHOICES = [2, 4]
+# DENSE numeric rows with >= 2^w products (and an output filling >= 1/16 of the
+# columns) take the column-window form; 0 = never
+WIN_DEFAULT = 17
+WIN_CHOICES = [0, 15, 17, 20]
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
 
 
 def default_tuning() -> dict:
-    return {"sym_lim": list(SYM_CAP), "num_lim": list(NUM_CAP), "hash_load": 2}
+    return {"sym_lim": list(SYM_CAP), "num_lim": list(NUM_CAP), "hash_load": 2, "dense_win_log2": WIN_DEFAULT}
 
 
 def valid(t: dict) -> bool:
@@ -49,6 +53,9 @@ def valid(t: dict) -> bool:
         for i in range(4):
             if v[i] < 1 or v[i] > cap[i] or (i and v[i] < v[i - 1]):
                 return False
+    w = t.get("dense_win_log2", WIN_DEFAULT)
+    if w != 0 and not 10 <= w <= 40:
+        return False
     return t["hash_load"] in (2, 4, 8)
 
 
@@ -57,11 +64,13 @@ def slots():
     out = [("sym_lim", i, opts) for i, opts in enumerate(SYM_CHOICES)]
     out += [("num_lim", i, opts) for i, opts in enumerate(NUM_CHOICES)]
     out.append(("hash_load", None, LOAD_CHOICES))
+    out.append(("dense_win_log2", None, WIN_CHOICES))
     return out
 
 
 def with_slot(t: dict, key: str, i, v) -> dict:
-    u = {"sym_lim": list(t["sym_lim"]), "num_lim": list(t["num_lim"]), "hash_load": t["hash_load"]}
+    u = {"sym_lim": list(t["sym_lim"]), "num_lim": list(t["num_lim"]), "hash_load": t["hash_load"],
+         "dense_win_log2": t.get("dense_win_log2", WIN_DEFAULT)}
     if i is None:
         u[key] = v
     else:
@@ -73,7 +82,7 @@ def neighbours(t: dict):
     """Every valid tuning that differs from t in one slot."""
     for key, i, opts in slots():
         for v in opts:
-            if v != (t[key] if i is None else t[key][i]):
+            if v != (t.get(key, WIN_DEFAULT) if i is None else t[key][i]):
                 u = with_slot(t, key, i, v)
                 if valid(u):
                     yield u
