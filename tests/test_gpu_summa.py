@@ -8,13 +8,13 @@ from trident_b200 import summa, workloads
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("use_masks", [True, False])
-def test_summa_4x4_rmat(ctx, use_masks):
+@pytest.mark.parametrize("use_masks,batched", [(True, False), (False, False), (True, True)])
+def test_summa_4x4_rmat(ctx, use_masks, batched):
     A = workloads.rmat(scale=11, edge_factor=8, seed=3)
     tiles, rb, cb = summa.cut_tiles(A, 4)
     dt = [[t.to_device() for t in row] for row in tiles]
     st = summa.StageStats()
-    C = summa.summa(ctx, dt, dt, 4, use_masks=use_masks, stats=st)
+    C = summa.summa(ctx, dt, dt, 4, use_masks=use_masks, stats=st, batched=batched)
     H = summa.assemble(C, rb, cb)
     rp, cj, cx, ca = oracle.spgemm(A, A)
     np.testing.assert_array_equal(H.rowptr, rp)

@@ -60,13 +60,21 @@ class StageStats:
     per_stage: list = field(default_factory=list)
 
 
-def summa(ctx, A_tiles, B_tiles, q: int, use_masks: bool = True, stats: StageStats | None = None):
-    """C tiles of A·B from device tiles A_tiles[i][k], B_tiles[k][j]."""
+def summa(ctx, A_tiles, B_tiles, q: int, use_masks: bool = True, stats: StageStats | None = None,
+          batched: bool = False):
+    """C tiles of A·B from device tiles A_tiles[i][k], B_tiles[k][j].
+
+    batched=True runs the q*q tile products of a stage as one batch (one
+    launch of each persistent kernel per phase, tspg_batch_*), then merges
+    every product into its C tile (tspg_spadd) — the split accumulate; the
+    default multiplies and accumulates tile by tile (tspg_spgemm_acc)."""
     C = [[None] * q for _ in range(q)]
+    batch = ops.Batch(ctx) if batched else None
     # per-tile CSC of A (what the reference keeps with --Acsc), packed by columns
     A_csc = [[ops.transpose(ctx, A_tiles[i][k]) for k in range(q)] for i in range(q)]
     for s in range(q):  # stage
         st = {"stage": s, "a_kept": 0, "b_kept": 0}
+        pairs = []
         for i in range(q):
             for j in range(q):
                 Aik, Bkj = A_tiles[i][s], B_tiles[s][j]
@@ -97,10 +105,29 @@ def summa(ctx, A_tiles, B_tiles, q: int, use_masks: bool = True, stats: StageSta
                     st["b_kept"] += bkept
                 else:
                     Ap, Bp = Aik, Bkj
-                C[i][j] = ops.sp_mma(ctx, Ap, Bp, C[i][j])
+                if batch is None:
+                    C[i][j] = ops.sp_mma(ctx, Ap, Bp, C[i][j])
+                else:
+                    pairs.append((i, j, Ap, Bp))
+        if batch is not None and pairs:
+            batch.clear()
+            for _, _, Ap, Bp in pairs:
+                batch.add(Ap, Bp)
+            batch.run()
+            for t, (i, j, _, _) in enumerate(pairs):
+                P = batch.result(t)
+                # the slab is rewritten by the next stage's run: merge (or copy) out now
+                C[i][j] = ops.spadd(ctx, P, C[i][j]) if C[i][j] is not None else _copy(P)
         if stats is not None:
             stats.per_stage.append(st)
+    if batch is not None:
+        batch.close()
     return C
+
+
+def _copy(M: DeviceCSR) -> DeviceCSR:
+    return DeviceCSR(M.nrows, M.ncols, M.rowptr.clone(), M.col[:max(M.nnz, 1)].clone(),
+                     M.val[:max(M.nnz, 1)].clone(), nnz=M.nnz)
 
 
 def assemble(C_tiles, rb, cb) -> HostCSR:
