@@ -412,8 +412,10 @@ int tspg_batch_result(const tspg_batch *b, int i, tspg_csr *out);
  * `lanes` worker threads (own context and stream) then admits from the head
  * of that FIFO, in submission order, the requests (up to max_batch) that fit
  * `mem_budget` bytes and runs them as one batched product per stage, so
- * batches formed while others run overlap on the device.  Results (int64 row
- * offsets) stay valid until release. */
+ * batches formed while others run overlap on the device.  A result (int64
+ * row offsets) is a view into the output slab of the batch that computed it,
+ * not a copy; it stays valid until release, and a batch is reused only once
+ * every request it computed has been released. */
 enum { TSPG_REQ_AB = 0, TSPG_REQ_RAP = 1 };
 typedef struct tspg_server tspg_server;
 typedef struct tspg_server_config {

@@ -11,9 +11,11 @@
 // requests run as one batched product per stage: stage 1 = all A·B requests
 // plus the A·P half of the R·A·P requests, stage 2 = R·(AP) for the R·A·P
 // requests.  Lanes run concurrently on their own streams, so a batch that
-// forms while others are on the device overlaps with them.  Results are copied
-// out of the batch slab into per-request buffers from the lane's pool, which
-// stay valid until tspg_server_release.
+// forms while others are on the device overlaps with them.  Results are not
+// copied: a request's result is its view into the output slab of the batch
+// that computed it, and the lane keeps that batch (a "group": the stage-1 and
+// stage-2 batches of one admission) out of use until every request of the
+// group is released; released groups go back to the lane for reuse.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -35,17 +37,19 @@
     if (st_ != TSPG_OK) return st_; \
   } while (0)
 
-namespace tspg {
-int ws_alloc(tspg_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
-void ws_free(tspg_ctx *ctx, void *p, cudaStream_t s);
-}  // namespace tspg
-
 namespace {
 
 double now_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
 }
+
+// The two batches of one admitted group and how many of its requests still
+// hold results in their slabs.
+struct Group {
+  tspg_batch *b1 = nullptr, *b2 = nullptr;
+  int live = 0;
+};
 
 struct Req {
   int64_t ticket = 0;
@@ -57,8 +61,9 @@ struct Req {
   double t_submit = 0, t_start = 0, t_done = 0;
   int status = TSPG_OK;
   bool done = false;
-  // result (device, from the owning lane's pool)
+  // result: a view into the output slab of its group's batch
   int lane = -1;
+  Group *group = nullptr;
   int64_t nrows = 0, ncols = 0, nnz = 0;
   int64_t *rp = nullptr;
   int32_t *col = nullptr;
@@ -83,6 +88,8 @@ struct tspg_server {
   cudaStream_t bstream = nullptr;
   std::vector<tspg_ctx *> lane_ctx;
   std::vector<cudaStream_t> lane_stream;
+  // per lane: every group it made, and the released ones ready for reuse
+  std::vector<std::vector<Group *>> lane_groups, lane_free;
   int64_t batches = 0, completed = 0, rejected = 0;
   int lane_error = TSPG_OK;
 };
@@ -103,29 +110,17 @@ size_t out_bytes(int64_t nnz_upper, int64_t rows, int vb) {
   return size_t(nnz_upper) * size_t(4 + vb) + size_t(rows + 1) * 8;
 }
 
-// Copy batch result i into request-owned buffers from the lane pool.
-int take_result(tspg_ctx *ctx, cudaStream_t s, tspg_batch *b, int i, Req *r, int vb) {
+// Point request r at batch result i (a view into the batch's output slab).
+int take_result(tspg_batch *b, int i, Req *r) {
   tspg_csr v{};
   int st = tspg_batch_result(b, i, &v);
   if (st != TSPG_OK) return st;
   r->nrows = v.nrows;
   r->ncols = v.ncols;
   r->nnz = v.nnz;
-  void *rp = nullptr, *col = nullptr, *val = nullptr;
-  st = tspg::ws_alloc(ctx, &rp, size_t(v.nrows + 1) * 8, s);
-  if (st == TSPG_OK) st = tspg::ws_alloc(ctx, &col, size_t(v.nnz > 0 ? v.nnz : 1) * 4, s);
-  if (st == TSPG_OK) st = tspg::ws_alloc(ctx, &val, size_t(v.nnz > 0 ? v.nnz : 1) * vb, s);
-  if (st != TSPG_OK) return st;
-  r->rp = (int64_t *)rp;
-  r->col = (int32_t *)col;
-  r->val = val;
-  if (cudaMemcpyAsync(rp, v.rowptr, size_t(v.nrows + 1) * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-    return TSPG_ECUDA;
-  if (v.nnz > 0) {
-    if (cudaMemcpyAsync(col, v.col, size_t(v.nnz) * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(val, v.val, size_t(v.nnz) * vb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-      return TSPG_ECUDA;
-  }
+  r->rp = (int64_t *)v.rowptr;
+  r->col = (int32_t *)v.col;
+  r->val = (void *)v.val;
   return TSPG_OK;
 }
 
@@ -210,12 +205,10 @@ void lane_main(tspg_server *S, int lane) {
   cudaSetDevice(S->device);
   tspg_ctx *ctx = S->lane_ctx[lane];
   cudaStream_t s = S->lane_stream[lane];
-  tspg_batch *b1 = nullptr, *b2 = nullptr;
-  tspg_batch_create(ctx, &b1);
-  tspg_batch_create(ctx, &b2);
   std::vector<Req *> take;
   while (true) {
     take.clear();
+    Group *g = nullptr;
     {
       std::unique_lock<std::mutex> lk(S->mu);
       S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty(); });
@@ -239,11 +232,35 @@ void lane_main(tspg_server *S, int lane) {
         S->cv_done.wait_for(lk, std::chrono::milliseconds(1));
         continue;
       }
+      if (!S->lane_free[lane].empty()) {
+        g = S->lane_free[lane].back();
+        S->lane_free[lane].pop_back();
+      }
     }
+    if (!g) {  // a new group (its batches hold the results until released)
+      g = new (std::nothrow) Group();
+      int cst = g ? tspg_batch_create(ctx, &g->b1) : TSPG_ENOMEM;
+      if (cst == TSPG_OK) cst = tspg_batch_create(ctx, &g->b2);
+      std::lock_guard<std::mutex> lk(S->mu);
+      if (g) S->lane_groups[lane].push_back(g);
+      if (cst != TSPG_OK) {
+        for (Req *r : take) {
+          r->status = cst;
+          r->done = true;
+          S->reserved -= r->reserve;
+          r->admitted = false;
+        }
+        S->lane_error = cst;
+        S->cv_done.notify_all();
+        if (g) S->lane_free[lane].push_back(g);
+        g = nullptr;
+        continue;
+      }
+    }
+    tspg_batch *b1 = g->b1, *b2 = g->b2;
     const double t0 = now_ms();
     for (Req *r : take) r->t_start = t0;
     int st = TSPG_OK;
-    int vb = take[0]->A.val_bits / 8;
     // stage 1: A·B and A·P
     tspg_batch_clear(b1);
     for (Req *r : take) {
@@ -269,9 +286,8 @@ void lane_main(tspg_server *S, int lane) {
     if (st == TSPG_OK) {
       for (int i = 0, k = 0; i < (int)take.size() && st == TSPG_OK; ++i) {
         Req *r = take[i];
-        if (r->kind == TSPG_REQ_RAP) st = take_result(ctx, s, b2, k++, r, vb);
-        else st = take_result(ctx, s, b1, i, r, vb);
-        r->lane = lane;
+        if (r->kind == TSPG_REQ_RAP) st = take_result(b2, k++, r);
+        else st = take_result(b1, i, r);
       }
     }
     if (cudaStreamSynchronize(s) != cudaSuccess && st == TSPG_OK) st = TSPG_ECUDA;
@@ -282,19 +298,22 @@ void lane_main(tspg_server *S, int lane) {
         r->status = st;
         r->t_done = t1;
         r->done = true;
+        r->lane = lane;
         if (st != TSPG_OK) {
           S->reserved -= r->reserve;
           r->admitted = false;
+        } else {
+          r->group = g;
         }
       }
+      if (st == TSPG_OK) g->live = int(take.size());
+      else S->lane_free[lane].push_back(g);  // nothing refers to its slabs
       S->batches += 1;
       S->completed += int64_t(take.size());
       if (st != TSPG_OK) S->lane_error = st;
     }
     S->cv_done.notify_all();
   }
-  tspg_batch_destroy(b1);
-  tspg_batch_destroy(b2);
 }
 
 }  // namespace
@@ -308,6 +327,8 @@ extern "C" int tspg_server_create(tspg_ctx *ctx, const tspg_server_config *cfg,
   tspg_server *S = new (std::nothrow) tspg_server();
   if (!S) return TSPG_ENOMEM;
   S->cfg = *cfg;
+  S->lane_groups.resize(cfg->lanes);
+  S->lane_free.resize(cfg->lanes);
   int dev = 0;
   cudaGetDevice(&dev);
   S->device = dev;
@@ -347,15 +368,13 @@ extern "C" int tspg_server_destroy(tspg_server *S) {
   for (auto &t : S->threads) t.join();
   cudaSetDevice(S->device);
   cudaDeviceSynchronize();
-  for (auto &kv : S->reqs) {
-    Req *r = kv.second;
-    if (r->lane >= 0) {
-      tspg::ws_free(S->lane_ctx[r->lane], r->rp, nullptr);
-      tspg::ws_free(S->lane_ctx[r->lane], r->col, nullptr);
-      tspg::ws_free(S->lane_ctx[r->lane], r->val, nullptr);
+  for (auto &kv : S->reqs) delete kv.second;  // their results live in the groups' slabs
+  for (auto &gs : S->lane_groups)
+    for (Group *g : gs) {
+      if (g->b1) tspg_batch_destroy(g->b1);
+      if (g->b2) tspg_batch_destroy(g->b2);
+      delete g;
     }
-    delete r;
-  }
   // every request in fresh / queue is also in reqs (freed above)
   for (size_t l = 0; l < S->lane_ctx.size(); ++l) {
     if (S->lane_stream[l]) cudaStreamDestroy(S->lane_stream[l]);
@@ -434,13 +453,9 @@ extern "C" int tspg_server_release(tspg_server *S, int64_t ticket) {
     r = it->second;
     S->reqs.erase(it);
     if (r->admitted) S->reserved -= r->reserve;
-  }
-  if (r->lane >= 0) {
-    // the lane's pool is stream-ordered on the lane stream; its work on these
-    // buffers finished before the request was marked done
-    tspg::ws_free(S->lane_ctx[r->lane], r->rp, S->lane_stream[r->lane]);
-    tspg::ws_free(S->lane_ctx[r->lane], r->col, S->lane_stream[r->lane]);
-    tspg::ws_free(S->lane_ctx[r->lane], r->val, S->lane_stream[r->lane]);
+    // the last release of a group hands its batches back to the lane (the
+    // lane's work on their slabs finished before the requests were done)
+    if (r->group && --r->group->live == 0) S->lane_free[r->lane].push_back(r->group);
   }
   delete r;
   S->cv_work.notify_all();
