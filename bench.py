@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--dense-win", type=int, default=None,
                    help="override the tuning's dense_win_log2 (0 = whole-row rank form for every DENSE row)")
+    p.add_argument("--dense-fill", type=int, default=None,
+                   help="override the tuning's dense_win_fill_log2 (window form when nnz(row) >= ncols / 2^fill)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -246,7 +248,11 @@ def run_ours(args, rank, world):
     cfg_tuning = apply_tuning(ctx, "rmat") if args.workload == "rmat" else None
     if args.dense_win is not None:
         ctx.set_tuning({"dense_win_log2": args.dense_win})
-    cfg_tuning = dict(cfg_tuning or {}, dense_win_log2=ctx.get_tuning()["dense_win_log2"])
+    if args.dense_fill is not None:
+        ctx.set_tuning({"dense_win_fill_log2": args.dense_fill})
+    cur = ctx.get_tuning()
+    cfg_tuning = dict(cfg_tuning or {}, dense_win_log2=cur["dense_win_log2"],
+                      dense_win_fill_log2=cur["dense_win_fill_log2"])
     A = cfg = None
     if rank == 0:
         A, cfg = make_workload(args)

@@ -148,17 +148,20 @@ int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
  * (2, 4 or 8).  Bounds must be positive, non-decreasing and at most the table
  * capacities sym <= {512, 2048, 4096, 24576}, num <= {256, 1024, 2048, 8192}
  * (the defaults); otherwise TSPG_EINVAL.  dense_win_log2: numeric DENSE
- * rows with at least 2^dense_win_log2 products (and sorted B rows) take the
+ * rows with at least 2^dense_win_log2 products, an output filling at least
+ * 1/2^dense_win_fill_log2 of the columns and sorted B rows take the
  * column-window form (a shared-memory FP64 accumulator per window of
- * columns, written to C once) instead of the whole-row rank form; 0 turns it
- * off; otherwise 10..40 (default 17).  Applies to calls made after it;
+ * columns, written to C once) instead of the whole-row rank form;
+ * dense_win_log2 = 0 turns it off, otherwise 10..40 (default 17);
+ * dense_win_fill_log2 0..12 (default 4).  Applies to calls made after it;
  * results do not depend on it. */
 typedef struct tspg_tuning {
   int32_t sym_lim[4];
   int32_t num_lim[4];
   int32_t hash_load;
   int32_t dense_win_log2;
-  int32_t reserved[2];
+  int32_t dense_win_fill_log2;
+  int32_t reserved;
 } tspg_tuning;
 int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t);
 int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t);

@@ -21,6 +21,7 @@ def test_neighbours_are_valid_and_differ_in_one_slot():
         diff += sum(a != b for a, b in zip(u["num_lim"], t["num_lim"]))
         diff += u["hash_load"] != t["hash_load"]
         diff += u["dense_win_log2"] != t["dense_win_log2"]
+        diff += u["dense_win_fill_log2"] != t["dense_win_fill_log2"]
         assert diff == 1
         seen += 1
     assert seen > 10

@@ -58,7 +58,8 @@ class TspgTuning(C.Structure):
         ("num_lim", C.c_int32 * 4),
         ("hash_load", C.c_int32),
         ("dense_win_log2", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("dense_win_fill_log2", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

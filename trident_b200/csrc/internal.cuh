@@ -28,10 +28,11 @@ struct Tune {
   int32_t sym[4];
   int32_t num[4];
   int32_t load;
-  int32_t win;  // log2 of the products from which DENSE numeric rows take the window form; 0 = never
-  int32_t pad[2];
+  int32_t win;   // log2 of the products from which DENSE numeric rows take the window form; 0 = never
+  int32_t fill;  // ... when their output also fills >= 1 / 2^fill of the columns
+  int32_t pad;
 };
-constexpr int32_t kDefaultWinLog2 = 17;
+constexpr int32_t kDefaultWinLog2 = 17, kDefaultWinFillLog2 = 4;
 
 // A tuning is valid when every bound is positive, non-decreasing over the
 // classes and within the table capacity of its class, and load is 2, 4 or 8.
@@ -43,6 +44,7 @@ inline bool tune_valid(const Tune &t) {
     if (i > 0 && (t.sym[i] < t.sym[i - 1] || t.num[i] < t.num[i - 1])) return false;
   }
   if (t.win != 0 && (t.win < 10 || t.win > 40)) return false;
+  if (t.fill < 0 || t.fill > 12) return false;
   return t.load == 2 || t.load == 4 || t.load == 8;
 }
 }  // namespace tspg
@@ -76,7 +78,8 @@ struct tspg_ctx {
                       int32_t(tspg::kNumLim256), int32_t(tspg::kNumLim1024)},
                      2,
                      tspg::kDefaultWinLog2,
-                     {0, 0}};
+                     tspg::kDefaultWinFillLog2,
+                     0};
 };
 
 namespace tspg {

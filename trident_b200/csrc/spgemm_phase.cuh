@@ -1220,7 +1220,7 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 }
 
 // DENSE numeric row, column-window form, for heavy rows with sorted B whose
-// output fills at least 1/16 of the columns.  The row's columns are swept in
+// output fills at least 1/2^fill of the columns (tuning; default 1/16).  The row's columns are swept in
 // windows of kWinCols; a window accumulates in a shared FP64 array indexed by
 // column — one shared atomic per product, and no bitmap: a slot that still
 // holds the bit pattern of -0.0 is empty, because every product is added as
@@ -1599,10 +1599,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       if constexpr (NUM) {
         const RowRef rr = decode_row(A, idx);
         const ProdDev<PT, VT> &P = prods[rr.p];
-        // heavy rows whose output fills >= 1/16 of the columns: column windows
+        // heavy rows whose output fills >= 1/2^fill of the columns: column windows
         const int win = A.S->tune.win;
         if (P.b_sorted && win > 0 && A.rowf[rr.g] >= (int64_t(1) << win) &&
-            int64_t(A.rowc[rr.g]) * 16 >= P.n)
+            (int64_t(A.rowc[rr.g]) << A.S->tune.fill) >= P.n)
           num_dense_win_row<PT, VT>(prods, A, idx, smem, gm);
         else if (P.n <= kRankMaxCols)
           num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm);

@@ -36,12 +36,15 @@ LOAD_CHOICES = [2, 4]
 # columns) take the column-window form; 0 = never
 WIN_DEFAULT = 17
 WIN_CHOICES = [0, 15, 17, 20]
+FILL_DEFAULT = 4
+FILL_CHOICES = [3, 4, 5, 6]
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
 
 
 def default_tuning() -> dict:
-    return {"sym_lim": list(SYM_CAP), "num_lim": list(NUM_CAP), "hash_load": 2, "dense_win_log2": WIN_DEFAULT}
+    return {"sym_lim": list(SYM_CAP), "num_lim": list(NUM_CAP), "hash_load": 2, "dense_win_log2": WIN_DEFAULT,
+            "dense_win_fill_log2": FILL_DEFAULT}
 
 
 def valid(t: dict) -> bool:
@@ -56,6 +59,8 @@ def valid(t: dict) -> bool:
     w = t.get("dense_win_log2", WIN_DEFAULT)
     if w != 0 and not 10 <= w <= 40:
         return False
+    if not 0 <= t.get("dense_win_fill_log2", FILL_DEFAULT) <= 12:
+        return False
     return t["hash_load"] in (2, 4, 8)
 
 
@@ -65,12 +70,17 @@ def slots():
     out += [("num_lim", i, opts) for i, opts in enumerate(NUM_CHOICES)]
     out.append(("hash_load", None, LOAD_CHOICES))
     out.append(("dense_win_log2", None, WIN_CHOICES))
+    out.append(("dense_win_fill_log2", None, FILL_CHOICES))
     return out
+
+
+_SCALAR_DEFAULT = {"hash_load": 2, "dense_win_log2": WIN_DEFAULT, "dense_win_fill_log2": FILL_DEFAULT}
 
 
 def with_slot(t: dict, key: str, i, v) -> dict:
     u = {"sym_lim": list(t["sym_lim"]), "num_lim": list(t["num_lim"]), "hash_load": t["hash_load"],
-         "dense_win_log2": t.get("dense_win_log2", WIN_DEFAULT)}
+         "dense_win_log2": t.get("dense_win_log2", WIN_DEFAULT),
+         "dense_win_fill_log2": t.get("dense_win_fill_log2", FILL_DEFAULT)}
     if i is None:
         u[key] = v
     else:
@@ -82,7 +92,7 @@ def neighbours(t: dict):
     """Every valid tuning that differs from t in one slot."""
     for key, i, opts in slots():
         for v in opts:
-            if v != (t.get(key, WIN_DEFAULT) if i is None else t[key][i]):
+            if v != (t.get(key, _SCALAR_DEFAULT[key]) if i is None else t[key][i]):
                 u = with_slot(t, key, i, v)
                 if valid(u):
                     yield u
