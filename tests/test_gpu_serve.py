@@ -1,21 +1,41 @@
 """GPU: the continuous-batching server.  Each result must be the same alone
-(a plain call) and in the mix (batched with other requests), within the FP64
-tolerance; requests that arrive while others run are admitted and complete."""
+(a plain call) and in the mix (batched with other requests): both equal the
+oracle's product, structure bit-exact and FP64 values within
+1e-12 * max(|y|, sum |a b|); requests that arrive while others run are
+admitted and complete."""
 import threading
 
 import numpy as np
 import pytest
 
+import oracle
 from helpers import TOL64, random_csr
 from trident_b200 import ops, workloads
+from trident_b200.synth import HostCSR
 
 pytestmark = pytest.mark.gpu
 
 
-def _same(P, Q):
-    np.testing.assert_array_equal(P.rowptr.astype(np.int64), Q.rowptr.astype(np.int64))
-    np.testing.assert_array_equal(P.col, Q.col)
-    assert np.all(np.abs(P.val - Q.val) <= TOL64 * np.maximum(np.abs(P.val), 1.0) * 64)
+def _ref_ab(A, B):
+    rp, cj, cx, ca = oracle.spgemm(A, B)
+    return rp, cj, cx, ca
+
+
+def _ref_rap(R, A, P):
+    """R·(A·P) by the oracle, with the error scale of the chained product:
+    sum_k |r_ik| * (sum |a p|)_kj."""
+    rp1, cj1, cx1, ca1 = oracle.spgemm(A, P)
+    rp, cj, cx, _ = oracle.spgemm(R, HostCSR(A.nrows, P.ncols, rp1, cj1, cx1))
+    Rabs = HostCSR(R.nrows, R.ncols, R.rowptr, R.col, np.abs(R.val))
+    _, _, scale, _ = oracle.spgemm(Rabs, HostCSR(A.nrows, P.ncols, rp1, cj1, ca1), with_abs=False)
+    return rp, cj, cx, scale
+
+
+def _same(H, ref):
+    rp, cj, cx, scale = ref
+    np.testing.assert_array_equal(H.rowptr.astype(np.int64), rp)
+    np.testing.assert_array_equal(H.col, cj)
+    assert np.all(np.abs(H.val - cx) <= TOL64 * np.maximum(np.abs(cx), scale))
 
 
 def test_server_mix_matches_alone(ctx):
@@ -24,8 +44,12 @@ def test_server_mix_matches_alone(ctx):
     raps = [workloads.galerkin_operands(n=side, pts=7, agg=2) for side in (12, 20)]
     dab = [(A.to_device(), B.to_device()) for A, B in ab]
     drap = [(R.to_device(), A.to_device(), P.to_device()) for R, A, P in raps]
-    alone_ab = [ops.spgemm(ctx, A, B).to_host() for A, B in dab]
-    alone_rap = [ops.spgemm(ctx, R, ops.spgemm(ctx, A, P)).to_host() for R, A, P in drap]
+    ref_ab = [_ref_ab(A, B) for A, B in ab]
+    ref_rap = [_ref_rap(R, A, P) for R, A, P in raps]
+    for (A, B), ref in zip(dab, ref_ab):  # alone
+        _same(ops.spgemm(ctx, A, B).to_host(), ref)
+    for (R, A, P), ref in zip(drap, ref_rap):
+        _same(ops.spgemm(ctx, R, ops.spgemm(ctx, A, P)).to_host(), ref)
     srv = ops.Server(ctx, mem_budget=8 << 30, lanes=2, max_batch=16)
     tickets = []
     lock = threading.Lock()
@@ -50,7 +74,7 @@ def test_server_mix_matches_alone(ctx):
     for kind, i, t in tickets:
         res, ms = srv.wait(t, timeout_ms=60000)
         lat.append(ms)
-        _same(res.to_host(), alone_ab[i] if kind == "ab" else alone_rap[i])
+        _same(res.to_host(), ref_ab[i] if kind == "ab" else ref_rap[i])  # in the mix
         srv.release(t)
     st = srv.stats()
     assert st["completed"] == len(tickets) and st["reserved"] == 0 and st["status"] == 0
@@ -72,7 +96,7 @@ def test_server_rejects_oversized_request(ctx):
     assert e.value.status == TSPG_ENOMEM
     srv.release(t_big)
     res, _ = srv.wait(t_small, timeout_ms=60000)
-    _same(res.to_host(), ops.spgemm(ctx, dS, dS).to_host())
+    _same(res.to_host(), _ref_ab(S, S))
     srv.release(t_small)
     st = srv.stats()
     assert st["completed"] == 1 and st["reserved"] == 0
@@ -106,7 +130,7 @@ def test_server_admits_in_submission_order_under_a_tight_budget(ctx):
     mults, upper = ops.spgemm_count(ctx, *dev[0])
     one = upper * 12 + 6001 * 8
     srv = ops.Server(ctx, mem_budget=int(3.5 * one), lanes=3, max_batch=16)
-    want = [ops.spgemm(ctx, A, B).to_host() for A, B in dev]
+    want = [_ref_ab(A, B) for A, B in ops_pairs]
     tickets = [(k % 4, srv.submit(*dev[k % 4])) for k in range(48)]
     for k, t in tickets:
         res, _ = srv.wait(t, timeout_ms=60000)
