@@ -60,6 +60,8 @@ def parse():
                    help="override the tuning's dense_win_log2 (0 = whole-row rank form for every DENSE row)")
     p.add_argument("--dense-fill", type=int, default=None,
                    help="override the tuning's dense_win_fill_log2 (window form when nnz(row) >= ncols / 2^fill)")
+    p.add_argument("--dense-cluster", type=int, default=None,
+                   help="override the tuning's dense_win_cluster (CTAs per cluster for the window form; 0 = one CTA)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     return p.parse_args()
@@ -250,9 +252,12 @@ def run_ours(args, rank, world):
         ctx.set_tuning({"dense_win_log2": args.dense_win})
     if args.dense_fill is not None:
         ctx.set_tuning({"dense_win_fill_log2": args.dense_fill})
+    if args.dense_cluster is not None:
+        ctx.set_tuning({"dense_win_cluster": args.dense_cluster})
     cur = ctx.get_tuning()
     cfg_tuning = dict(cfg_tuning or {}, dense_win_log2=cur["dense_win_log2"],
-                      dense_win_fill_log2=cur["dense_win_fill_log2"])
+                      dense_win_fill_log2=cur["dense_win_fill_log2"],
+                      dense_win_cluster=cur["dense_win_cluster"])
     A = cfg = None
     if rank == 0:
         A, cfg = make_workload(args)

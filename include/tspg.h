@@ -153,15 +153,18 @@ int tspg_ctx_phase_ms(tspg_ctx *ctx, float *symbolic_ms, float *numeric_ms);
  * column-window form (a shared-memory FP64 accumulator per window of
  * columns, written to C once) instead of the whole-row rank form;
  * dense_win_log2 = 0 turns it off, otherwise 10..40 (default 17);
- * dense_win_fill_log2 0..12 (default 4).  Applies to calls made after it;
- * results do not depend on it. */
+ * dense_win_fill_log2 0..12 (default 4).  dense_win_cluster: 0 (default) —
+ * one CTA per such row; 2, 4 or 8 — a thread-block cluster of that many CTAs
+ * per row, the window spread over their shared memories (distributed shared
+ * memory) so it spans that many times the columns.  Applies to calls made
+ * after it; results do not depend on it. */
 typedef struct tspg_tuning {
   int32_t sym_lim[4];
   int32_t num_lim[4];
   int32_t hash_load;
   int32_t dense_win_log2;
   int32_t dense_win_fill_log2;
-  int32_t reserved;
+  int32_t dense_win_cluster;
 } tspg_tuning;
 int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t);
 int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t);

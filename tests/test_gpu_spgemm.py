@@ -278,13 +278,16 @@ def _window_operands(val_dtype=np.float64):
     return A, B
 
 
-@pytest.mark.parametrize("win", [10, 0])
-def test_dense_window_form(win):
-    """The column-window form (win = 10) and the rank form (win = 0) on the
-    same heavy rows: both equal the oracle (structure bit-exact, values within
-    1e-12), including the exact cancellation and the -0.0 product."""
+@pytest.mark.parametrize("win,cluster", [(10, 0), (10, 2), (10, 4), (0, 0)])
+def test_dense_window_form(win, cluster):
+    """The column-window form (win = 10) in one CTA per row and on clusters of
+    2 and 4 CTAs (the window in their distributed shared memory), and the rank
+    form (win = 0), on the same heavy rows: all equal the oracle (structure
+    bit-exact, values within 1e-12), including the exact cancellation and the
+    -0.0 product."""
     c = ops.Context(0)
-    c.set_tuning({"dense_win_log2": win, "num_lim": [1, 1, 1, 1], "sym_lim": [1, 1, 1, 1]})
+    c.set_tuning({"dense_win_log2": win, "dense_win_cluster": cluster, "num_lim": [1, 1, 1, 1],
+                  "sym_lim": [1, 1, 1, 1]})
     A, B = _window_operands()
     H = check_product(ops.spgemm(c, A.to_device(), B.to_device(), flags=TSPG_F_B_SORTED), A, B)
     r = A.nrows - 1
@@ -295,12 +298,14 @@ def test_dense_window_form(win):
     c.close()
 
 
-def test_dense_window_form_fp32_and_addend():
+@pytest.mark.parametrize("cluster", [0, 2])
+def test_dense_window_form_fp32_and_addend(cluster):
     """FP32 twin, and the fused accumulate (the addend's entries join every
-    window)."""
+    window), in one CTA and on a cluster."""
     from trident_b200._lib import TSPG_F_ACC_FUSE
     c = ops.Context(0)
-    c.set_tuning({"dense_win_log2": 10, "num_lim": [1, 1, 1, 1], "sym_lim": [1, 1, 1, 1]})
+    c.set_tuning({"dense_win_log2": 10, "dense_win_cluster": cluster, "num_lim": [1, 1, 1, 1],
+                  "sym_lim": [1, 1, 1, 1]})
     A, B = _window_operands(np.float32)
     C32 = ops.spgemm(c, A.to_device(val_bits=32), B.to_device(val_bits=32), flags=TSPG_F_B_SORTED)
     check_product(C32, A, B, tol=TOL32)

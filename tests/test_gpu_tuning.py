@@ -9,9 +9,9 @@ from trident_b200._lib import TSPG_EINVAL, TspgError
 pytestmark = pytest.mark.gpu
 
 TUNINGS = [
-    {"sym_lim": [128, 1024, 2048, 8192], "num_lim": [128, 512, 1024, 4096], "hash_load": 4, "dense_win_log2": 17, "dense_win_fill_log2": 4},
-    {"sym_lim": [512, 512, 512, 512], "num_lim": [256, 256, 256, 256], "hash_load": 2, "dense_win_log2": 0, "dense_win_fill_log2": 4},
-    {"sym_lim": [1, 1, 1, 1], "num_lim": [1, 1, 1, 1], "hash_load": 8, "dense_win_log2": 10, "dense_win_fill_log2": 12},
+    {"sym_lim": [128, 1024, 2048, 8192], "num_lim": [128, 512, 1024, 4096], "hash_load": 4, "dense_win_log2": 17, "dense_win_fill_log2": 4, "dense_win_cluster": 0},
+    {"sym_lim": [512, 512, 512, 512], "num_lim": [256, 256, 256, 256], "hash_load": 2, "dense_win_log2": 0, "dense_win_fill_log2": 4, "dense_win_cluster": 0},
+    {"sym_lim": [1, 1, 1, 1], "num_lim": [1, 1, 1, 1], "hash_load": 8, "dense_win_log2": 10, "dense_win_fill_log2": 12, "dense_win_cluster": 2},
 ]
 
 

@@ -22,6 +22,7 @@ def test_neighbours_are_valid_and_differ_in_one_slot():
         diff += u["hash_load"] != t["hash_load"]
         diff += u["dense_win_log2"] != t["dense_win_log2"]
         diff += u["dense_win_fill_log2"] != t["dense_win_fill_log2"]
+        diff += u["dense_win_cluster"] != t["dense_win_cluster"]
         assert diff == 1
         seen += 1
     assert seen > 10

@@ -59,7 +59,7 @@ class TspgTuning(C.Structure):
         ("hash_load", C.c_int32),
         ("dense_win_log2", C.c_int32),
         ("dense_win_fill_log2", C.c_int32),
-        ("reserved", C.c_int32),
+        ("dense_win_cluster", C.c_int32),
     ]
 
 

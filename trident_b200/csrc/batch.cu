@@ -18,7 +18,7 @@
 #include <new>
 #include <vector>
 
-#include "spgemm_phase.cuh"
+#include "spgemm_cluster.cuh"
 
 namespace tspg {
 
@@ -225,6 +225,10 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_groups<PT, VT, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupDynSmem));
+  // the cluster form must be launchable before it is captured (k_phase leaves
+  // its rows alone)
+  if (ctx->tune.cluster && cluster_slots<PT, VT>(ctx->device, ctx->tune.cluster) <= 0)
+    return TSPG_EINVAL;
   // the graphs hold the row binning of their capture: a new tuning re-captures
   const bool retune = std::memcmp(&b->tune, &ctx->tune, sizeof(Tune)) != 0;
   const bool rebuild = b->dirty || !b->g1 || b->gstream != s || retune;
@@ -414,12 +418,13 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       PhaseArgs pa{b->d_base, b->sched + 1, b->list, b->rowf, b->rowc, b->cp,
                    b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
       phase_mark(ctx, 1, 0, s);
+      launch_dense_cluster<PT, VT>(ctx, s, prods, pa);  // launchable: checked above
       k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
       k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 1, 1, s);
     }
     k_zero_rowptr<PT, VT><<<(nprod + 31) / 32, 32, 0, s>>>(prods, nprod);
-    b->g2_kernels = 2 + (R > 0 ? 4 : 0);
+    b->g2_kernels = 2 + (R > 0 ? 4 + (ctx->tune.cluster ? 1 : 0) : 0);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (e != cudaSuccess) {
       ctx->last_cuda = (int)e;

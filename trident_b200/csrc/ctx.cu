@@ -184,6 +184,7 @@ extern "C" int tspg_ctx_set_tuning(tspg_ctx *ctx, const tspg_tuning *t) {
   u.load = t->hash_load;
   u.win = t->dense_win_log2;
   u.fill = t->dense_win_fill_log2;
+  u.cluster = t->dense_win_cluster;
   if (!tune_valid(u)) return TSPG_EINVAL;
   ctx->tune = u;
   return TSPG_OK;
@@ -198,7 +199,7 @@ extern "C" int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t) {
   t->hash_load = ctx->tune.load;
   t->dense_win_log2 = ctx->tune.win;
   t->dense_win_fill_log2 = ctx->tune.fill;
-  t->reserved = 0;
+  t->dense_win_cluster = ctx->tune.cluster;
   return TSPG_OK;
 }
 

@@ -30,7 +30,7 @@ struct Tune {
   int32_t load;
   int32_t win;   // log2 of the products from which DENSE numeric rows take the window form; 0 = never
   int32_t fill;  // ... when their output also fills >= 1 / 2^fill of the columns
-  int32_t pad;
+  int32_t cluster;  // CTAs per thread-block cluster working on one such row (0 = one CTA)
 };
 constexpr int32_t kDefaultWinLog2 = 17, kDefaultWinFillLog2 = 4;
 
@@ -45,6 +45,7 @@ inline bool tune_valid(const Tune &t) {
   }
   if (t.win != 0 && (t.win < 10 || t.win > 40)) return false;
   if (t.fill < 0 || t.fill > 12) return false;
+  if (t.cluster != 0 && t.cluster != 2 && t.cluster != 4 && t.cluster != 8) return false;
   return t.load == 2 || t.load == 4 || t.load == 8;
 }
 }  // namespace tspg

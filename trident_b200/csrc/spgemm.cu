@@ -11,7 +11,7 @@
 #include <algorithm>
 #include <new>
 
-#include "spgemm_phase.cuh"
+#include "spgemm_cluster.cuh"
 
 namespace tspg {
 
@@ -205,6 +205,7 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
                P->curbuf, P->cur_stride, ctx->d_words + kErrWord,
                ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
   phase_mark(ctx, 1, 0, s);
+  TSPG_CUDA(ctx, launch_dense_cluster<PT, VT>(ctx, s, prods, pa));
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
   k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
   phase_mark(ctx, 1, 1, s);

@@ -145,7 +145,8 @@ struct Sched {
   int64_t upper;      // sum of min(mults, ncols)
   int64_t max_a_row;  // longest A row (sizes the DENSE cursor scratch)
   int64_t nonempty;
-  int64_t pad[3];
+  unsigned long long work2;  // row counter of the cluster kernel (column-window rows)
+  int64_t pad[2];
 };
 
 __device__ __forceinline__ int find_prod(const int64_t *base, int nprod,
@@ -321,6 +322,7 @@ static __global__ void k_sched_offsets(Sched *S) {
       o += S->cnt[c];
     }
     S->work = 0;
+    S->work2 = 0;
   }
 }
 

@@ -1237,6 +1237,13 @@ __device__ void num_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 // 1/16 of the window, takes 32 slots per step, keeps the step ballots in
 // registers (lane s holds step s), and a scan of the 16 warp counts places its
 // entries.
+// The rows the column-window form takes: heavy (>= 2^win products) DENSE rows
+// with sorted B whose output fills >= 1/2^fill of the columns.
+template <typename PT, typename VT>
+__device__ __forceinline__ bool win_row(const ProdDev<PT, VT> &P, int64_t f, int64_t c, const Tune &t) {
+  return P.b_sorted && t.win > 0 && f >= (int64_t(1) << t.win) && (c << t.fill) >= P.n;
+}
+
 constexpr int kWinCols = 16384;   // columns per window (128 KiB of FP64)
 constexpr int kWinQueue = 4096;   // queued long segments per window
 static_assert(kWinCols * 8 + 2 * kDenseCurSmem * 4 + kWinQueue * 4 <= kDynSmem, "window smem");
@@ -1599,12 +1606,12 @@ __global__ void __launch_bounds__(kThreads, 1)
       if constexpr (NUM) {
         const RowRef rr = decode_row(A, idx);
         const ProdDev<PT, VT> &P = prods[rr.p];
-        // heavy rows whose output fills >= 1/2^fill of the columns: column windows
-        const int win = A.S->tune.win;
-        if (P.b_sorted && win > 0 && A.rowf[rr.g] >= (int64_t(1) << win) &&
-            (int64_t(A.rowc[rr.g]) << A.S->tune.fill) >= P.n)
-          num_dense_win_row<PT, VT>(prods, A, idx, smem, gm);
-        else if (P.n <= kRankMaxCols)
+        // heavy rows whose output fills >= 1/2^fill of the columns: column
+        // windows, in this CTA or (tune.cluster > 0) in the cluster kernel
+        // that ran before this one
+        if (win_row(P, A.rowf[rr.g], int64_t(A.rowc[rr.g]), A.S->tune)) {
+          if (A.S->tune.cluster == 0) num_dense_win_row<PT, VT>(prods, A, idx, smem, gm);
+        } else if (P.n <= kRankMaxCols)
           num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm);
         else
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);

@@ -65,18 +65,19 @@ class Context:
 
     def get_tuning(self) -> dict:
         """Row binning in force: {"sym_lim": [4], "num_lim": [4], "hash_load": k,
-        "dense_win_log2": w, "dense_win_fill_log2": d}."""
+        "dense_win_log2": w, "dense_win_fill_log2": d, "dense_win_cluster": k}."""
         t = TspgTuning()
         check(lib.tspg_ctx_get_tuning(self.h, C.byref(t)), "tspg_ctx_get_tuning")
         return {"sym_lim": list(t.sym_lim), "num_lim": list(t.num_lim), "hash_load": t.hash_load,
-                "dense_win_log2": t.dense_win_log2, "dense_win_fill_log2": t.dense_win_fill_log2}
+                "dense_win_log2": t.dense_win_log2, "dense_win_fill_log2": t.dense_win_fill_log2,
+                "dense_win_cluster": t.dense_win_cluster}
 
     def set_tuning(self, tuning: dict):
         """Set the row binning (keys as get_tuning returns; missing keys keep
         their current values).  Raises TspgError(TSPG_EINVAL) when a bound is
         out of range."""
         cur = self.get_tuning()
-        keys = ("sym_lim", "num_lim", "hash_load", "dense_win_log2", "dense_win_fill_log2")
+        keys = ("sym_lim", "num_lim", "hash_load", "dense_win_log2", "dense_win_fill_log2", "dense_win_cluster")
         cur.update({k: tuning[k] for k in keys if k in tuning})
         t = TspgTuning()
         for i in range(4):
@@ -85,6 +86,7 @@ class Context:
         t.hash_load = int(cur["hash_load"])
         t.dense_win_log2 = int(cur["dense_win_log2"])
         t.dense_win_fill_log2 = int(cur["dense_win_fill_log2"])
+        t.dense_win_cluster = int(cur["dense_win_cluster"])
         check(lib.tspg_ctx_set_tuning(self.h, C.byref(t)), "tspg_ctx_set_tuning")
 
     def load_tuning(self, path: str) -> dict:

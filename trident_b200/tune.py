@@ -38,13 +38,15 @@ WIN_DEFAULT = 17
 WIN_CHOICES = [0, 15, 17, 20]
 FILL_DEFAULT = 4
 FILL_CHOICES = [3, 4, 5, 6]
+CLUSTER_DEFAULT = 0
+CLUSTER_CHOICES = [0, 2, 4]
 
 TUNING_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning")
 
 
 def default_tuning() -> dict:
     return {"sym_lim": list(SYM_CAP), "num_lim": list(NUM_CAP), "hash_load": 2, "dense_win_log2": WIN_DEFAULT,
-            "dense_win_fill_log2": FILL_DEFAULT}
+            "dense_win_fill_log2": FILL_DEFAULT, "dense_win_cluster": CLUSTER_DEFAULT}
 
 
 def valid(t: dict) -> bool:
@@ -61,6 +63,8 @@ def valid(t: dict) -> bool:
         return False
     if not 0 <= t.get("dense_win_fill_log2", FILL_DEFAULT) <= 12:
         return False
+    if t.get("dense_win_cluster", CLUSTER_DEFAULT) not in (0, 2, 4, 8):
+        return False
     return t["hash_load"] in (2, 4, 8)
 
 
@@ -71,16 +75,19 @@ def slots():
     out.append(("hash_load", None, LOAD_CHOICES))
     out.append(("dense_win_log2", None, WIN_CHOICES))
     out.append(("dense_win_fill_log2", None, FILL_CHOICES))
+    out.append(("dense_win_cluster", None, CLUSTER_CHOICES))
     return out
 
 
-_SCALAR_DEFAULT = {"hash_load": 2, "dense_win_log2": WIN_DEFAULT, "dense_win_fill_log2": FILL_DEFAULT}
+_SCALAR_DEFAULT = {"hash_load": 2, "dense_win_log2": WIN_DEFAULT, "dense_win_fill_log2": FILL_DEFAULT,
+                   "dense_win_cluster": CLUSTER_DEFAULT}
 
 
 def with_slot(t: dict, key: str, i, v) -> dict:
     u = {"sym_lim": list(t["sym_lim"]), "num_lim": list(t["num_lim"]), "hash_load": t["hash_load"],
          "dense_win_log2": t.get("dense_win_log2", WIN_DEFAULT),
-         "dense_win_fill_log2": t.get("dense_win_fill_log2", FILL_DEFAULT)}
+         "dense_win_fill_log2": t.get("dense_win_fill_log2", FILL_DEFAULT),
+         "dense_win_cluster": t.get("dense_win_cluster", CLUSTER_DEFAULT)}
     if i is None:
         u[key] = v
     else:
