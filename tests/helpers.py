@@ -51,3 +51,31 @@ def check_sum(C, A, B, tol=TOL64):
     np.testing.assert_array_equal(H.col, cj)
     np.testing.assert_allclose(H.val, cx, rtol=tol, atol=tol)
     return H
+
+
+def spgemm_poisoned(ctx, A, B, flags=0):
+    """C = A·B through the C ABI into output arrays pre-filled with garbage
+    (row offsets -3, columns -7, values NaN), so an entry the kernels fail to
+    write cannot pass for a stale result of an earlier call that the caching
+    allocator handed back."""
+    import ctypes as C
+
+    import torch
+
+    from trident_b200 import ops
+    from trident_b200._lib import TspgCsrOut, check, lib
+    from trident_b200.csr import DeviceCSR
+    plan = ops.Plan(ctx, A, B, flags)
+    nnz = plan.c_nnz
+    plan.close()
+    rp = torch.full((A.nrows + 1,), -3, dtype=torch.int64, device="cuda")
+    col = torch.full((max(nnz, 1),), -7, dtype=torch.int32, device="cuda")
+    val = torch.full((max(nnz, 1),), float("nan"), dtype=A.val.dtype, device="cuda")
+    o = TspgCsrOut()
+    o.nrows, o.ncols = A.nrows, B.ncols
+    o.rowptr, o.rowptr_bits, o.val_bits = rp.data_ptr(), 64, A.val_bits
+    o.col, o.val, o.capacity = col.data_ptr(), val.data_ptr(), nnz
+    a, b = A.abi(), B.abi()
+    check(lib.tspg_spgemm(ctx.h, torch.cuda.current_stream().cuda_stream, C.byref(a), C.byref(b), C.byref(o),
+                          flags), "tspg_spgemm")
+    return DeviceCSR(A.nrows, B.ncols, rp, col, val, nnz=nnz)

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 import oracle
-from helpers import TOL32, check_product, random_csr
+from helpers import TOL32, check_product, random_csr, spgemm_poisoned
 from trident_b200 import ops, workloads
 from trident_b200._lib import TSPG_EINVAL, TSPG_F_B_SORTED, TspgError
 from trident_b200.csr import HostCSR
@@ -289,7 +289,7 @@ def test_dense_window_form(win, cluster):
     c.set_tuning({"dense_win_log2": win, "dense_win_cluster": cluster, "num_lim": [1, 1, 1, 1],
                   "sym_lim": [1, 1, 1, 1]})
     A, B = _window_operands()
-    H = check_product(ops.spgemm(c, A.to_device(), B.to_device(), flags=TSPG_F_B_SORTED), A, B)
+    H = check_product(spgemm_poisoned(c, A.to_device(), B.to_device(), flags=TSPG_F_B_SORTED), A, B)
     r = A.nrows - 1
     row = H.col[H.rowptr[r]:H.rowptr[r + 1]]
     assert 7 in row and H.val[H.rowptr[r] + int(np.searchsorted(row, 7))] == 0.0
@@ -307,9 +307,11 @@ def test_dense_window_form_fp32_and_addend(cluster):
     c.set_tuning({"dense_win_log2": 10, "dense_win_cluster": cluster, "num_lim": [1, 1, 1, 1],
                   "sym_lim": [1, 1, 1, 1]})
     A, B = _window_operands(np.float32)
-    C32 = ops.spgemm(c, A.to_device(val_bits=32), B.to_device(val_bits=32), flags=TSPG_F_B_SORTED)
+    C32 = spgemm_poisoned(c, A.to_device(val_bits=32), B.to_device(val_bits=32), flags=TSPG_F_B_SORTED)
     check_product(C32, A, B, tol=TOL32)
     E = random_csr(A.nrows, B.ncols, per_row=3000, seed=31)
+    junk = torch.full((8 << 20,), -7, dtype=torch.int64, device="cuda")  # blocks the allocator hands back
+    del junk
     D = ops.sp_mma(c, A.to_device(), B.to_device(), E.to_device(), flags=TSPG_F_ACC_FUSE)
     rp, cj, cx, ca = oracle.spgemm(A, B)
     S = oracle.spadd(HostCSR(A.nrows, B.ncols, rp, cj, cx), E)

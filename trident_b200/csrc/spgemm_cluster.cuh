@@ -75,8 +75,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   int32_t *nxc_s = cur_s + kDenseCurSmem;
   int32_t *queue = nxc_s + kDenseCurSmem;
   const Tune t = A.S->tune;
-  const int64_t n_items = A.S->cnt[CLS_DENSE0] + A.S->cnt[CLS_DENSE1];
-  const int64_t list0 = A.S->off[CLS_DENSE0];  // DENSE0 then DENSE1, contiguous
+  // every DENSE class (DENSE0, DENSE1, DENSE2: contiguous in the list); the
+  // window rule, not the class, decides which rows are taken
+  const int64_t n_items = A.S->cnt[CLS_DENSE0] + A.S->cnt[CLS_DENSE1] + A.S->cnt[CLS_DENSE2];
+  const int64_t list0 = A.S->off[CLS_DENSE0];
   const uint32_t acc_u32 = smem_u32(acc);
   const uint64_t pass = policy_evict_first();
   for (int i = tid; i < kWinCols; i += kThreads) accb[i] = kEmpty;
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             if (unsigned(cc[u] - w0i) < wlen) {
-              add(cc[u], a * xv[u] + VT(0));
+              add(cc[u], win_value(a * xv[u]));
               ++nin;
             }
           }
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         addend_row(P, rr.r, e0, e1);
         for (int64_t e = e0 + int64_t(rank) + int64_t(tid) * K; e < e1; e += int64_t(kThreads) * K) {
           const int32_t col = __ldg(P.Ej + e);
-          if (col >= w0 && col < w1) add(col, __ldg(P.Ex + e) + VT(0));
+          if (col >= w0 && col < w1) add(col, win_value(__ldg(P.Ex + e)));
         }
       }
       __syncthreads();
@@ -217,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             if (unsigned(cc[u] - w0i) < wlen) {
-              add(cc[u], a * xv[u] + VT(0));
+              add(cc[u], win_value(a * xv[u]));
               ++nin;
             }
           }

@@ -1244,6 +1244,17 @@ __device__ __forceinline__ bool win_row(const ProdDev<PT, VT> &P, int64_t f, int
   return P.b_sorted && t.win > 0 && f >= (int64_t(1) << t.win) && (c << t.fill) >= P.n;
 }
 
+// A product as the window forms add it: never -0.0, so that an accumulator
+// slot still holding -0.0 is known to be empty.  Zeros and subnormals are
+// added as +0.0 (float atomics flush subnormal operands to a zero of the same
+// sign, so a negative subnormal could otherwise arrive as -0.0; the change is
+// below the smallest normal number, 1.2e-38 in FP32, 2.2e-308 in FP64).
+template <typename VT>
+__device__ __forceinline__ VT win_value(VT v) {
+  if constexpr (sizeof(VT) == 4) return fabsf(v) < 1.17549435e-38f ? 0.0f : v;
+  else return fabs(v) < 2.2250738585072014e-308 ? 0.0 : v;
+}
+
 constexpr int kWinCols = 16384;   // columns per window (128 KiB of FP64)
 constexpr int kWinQueue = 4096;   // queued long segments per window
 static_assert(kWinCols * 8 + 2 * kDenseCurSmem * 4 + kWinQueue * 4 <= kDynSmem, "window smem");
@@ -1322,7 +1333,7 @@ __device__ void num_dense_win_row(const ProdDev<PT, VT> *prods, const PhaseArgs 
           // possible when B's rows are not sorted as promised — is skipped,
           // never written out of bounds)
           if (unsigned(cc[u] - w0i) < wlen) {
-            atomicAdd(acc + (cc[u] - w0i), a * xv[u] + VT(0));
+            atomicAdd(acc + (cc[u] - w0i), win_value(a * xv[u]));
             ++nin;
           }
         }
@@ -1350,7 +1361,7 @@ __device__ void num_dense_win_row(const ProdDev<PT, VT> *prods, const PhaseArgs 
     }
     // the addend row of the accumulate form: every window takes its columns
     for_addend<true>(P, rr.r, tid, kThreads, [&](int32_t col, VT v) {
-      if (col >= w0 && col < w1) atomicAdd(acc + (col - w0i), v + VT(0));
+      if (col >= w0 && col < w1) atomicAdd(acc + (col - w0i), win_value(v));
     });
     __syncthreads();
     prof_sub(A, 6, tp);
@@ -1378,7 +1389,7 @@ __device__ void num_dense_win_row(const ProdDev<PT, VT> *prods, const PhaseArgs 
           // possible when B's rows are not sorted as promised — is skipped,
           // never written out of bounds)
           if (unsigned(cc[u] - w0i) < wlen) {
-            atomicAdd(acc + (cc[u] - w0i), a * xv[u] + VT(0));
+            atomicAdd(acc + (cc[u] - w0i), win_value(a * xv[u]));
             ++nin;
           }
         }
