@@ -139,10 +139,10 @@ def make_workload(args):
     return A, cfg
 
 
-def sample_rows(A, mults_total, target=2.5e9):
+def sample_rows(A, mults_total, target=6e9):
     """The CPU sample of a workload: rows i = 1 mod s of A (all rows when
     s = 1), s the smallest power of two that keeps the sample at or below
-    `target` multiply-adds (about 5 s of the oracle on 16 host cores).  The
+    `target` multiply-adds (about 10 s of the oracle on 16 host cores).  The
     timed CPU baseline, the reference arm and the parity check all use it."""
     import numpy as np
     s = 1

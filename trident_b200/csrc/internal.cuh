@@ -32,7 +32,7 @@ struct Tune {
   int32_t fill;  // ... when their output also fills >= 1 / 2^fill of the columns
   int32_t cluster;  // CTAs per thread-block cluster working on one such row (0 = one CTA)
 };
-constexpr int32_t kDefaultWinLog2 = 17, kDefaultWinFillLog2 = 4;
+constexpr int32_t kDefaultWinLog2 = 0, kDefaultWinFillLog2 = 4;  // window form off by default (measured slower)
 
 // A tuning is valid when every bound is positive, non-decreasing over the
 // classes and within the table capacity of its class, and load is 2, 4 or 8.

@@ -34,8 +34,8 @@ NUM_CHOICES = [[128, 192, 256], [512, 768, 1024], [1024, 1536, 2048], [4096, 614
 LOAD_CHOICES = [2, 4]
 # DENSE numeric rows with >= 2^w products (and an output filling >= 1/16 of the
 # columns) take the column-window form; 0 = never
-WIN_DEFAULT = 17
-WIN_CHOICES = [0, 15, 17, 20]
+WIN_DEFAULT = 0
+WIN_CHOICES = [0, 17, 20]
 FILL_DEFAULT = 4
 FILL_CHOICES = [3, 4, 5, 6]
 CLUSTER_DEFAULT = 0
