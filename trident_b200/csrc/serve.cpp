@@ -241,8 +241,13 @@ void lane_main(tspg_server *S, int lane) {
       g = new (std::nothrow) Group();
       int cst = g ? tspg_batch_create(ctx, &g->b1) : TSPG_ENOMEM;
       if (cst == TSPG_OK) cst = tspg_batch_create(ctx, &g->b2);
+      if (cst != TSPG_OK && g) {  // a partial group is not kept
+        if (g->b1) tspg_batch_destroy(g->b1);
+        if (g->b2) tspg_batch_destroy(g->b2);
+        delete g;
+        g = nullptr;
+      }
       std::lock_guard<std::mutex> lk(S->mu);
-      if (g) S->lane_groups[lane].push_back(g);
       if (cst != TSPG_OK) {
         for (Req *r : take) {
           r->status = cst;
@@ -252,10 +257,9 @@ void lane_main(tspg_server *S, int lane) {
         }
         S->lane_error = cst;
         S->cv_done.notify_all();
-        if (g) S->lane_free[lane].push_back(g);
-        g = nullptr;
         continue;
       }
+      S->lane_groups[lane].push_back(g);
     }
     tspg_batch *b1 = g->b1, *b2 = g->b2;
     const double t0 = now_ms();
