@@ -106,12 +106,59 @@ __device__ __forceinline__ void for_products_balanced(
   }
 }
 
+// One chunk of at most 32 A entries of a warp row: lane j holds entry j's
+// value a and B row bounds [b0, b0 + len) (len = 0 past the chunk's nc
+// entries); fn(col, a*b) for every product.  A warp scan numbers the chunk's
+// products and lanes take products lane, lane + 32, ... (U per step, loads in
+// flight), each finding its entry by a 5-step shuffle search.  (Lane j
+// walking entry j's B row itself, with no search, measured slower on the
+// Galerkin A·P rows, 27 entries x ~4.5: symbolic 2.35 vs 1.81 ms, numeric
+// 5.35 vs 3.72 ms — each load touches 32 B rows instead of a few, and lanes
+// whose B rows list the same columns hit them in the same step.)
+template <bool NUM, typename IX, typename VT, typename F>
+__device__ __forceinline__ void warp_chunk(const int32_t *__restrict__ Bj,
+                                           const VT *__restrict__ Bx, IX b0, IX len, VT a,
+                                           int nc, int lane, F &&fn) {
+  constexpr int U = 4;
+  const IX inc = warp_scan_incl(len);
+  const IX tot = __shfl_sync(0xffffffffu, inc, 31);
+  const IX pre = inc - len;
+  // the step loop is uniform across the warp (the search shuffles)
+  for (IX pb = 0; pb < tot; pb += IX(32) * U) {
+    int32_t cc[U];
+    VT xv[U], av[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const IX p = pb + IX(u) * 32 + lane;
+      int j = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const IX v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
+        if (j + st < nc && v <= p) j += st;
+      }
+      const IX pj = __shfl_sync(0xffffffffu, pre, j);
+      const IX bj = __shfl_sync(0xffffffffu, b0, j);
+      if constexpr (NUM) av[u] = __shfl_sync(0xffffffffu, a, j);
+      const IX q = bj + (p - pj);
+      cc[u] = p < tot ? __ldg(Bj + q) : -1;
+      if constexpr (NUM) xv[u] = p < tot ? __ldg(Bx + q) : VT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (cc[u] >= 0) {
+        if constexpr (NUM) fn(cc[u], av[u] * xv[u]);
+        else fn(cc[u], VT(0));
+      }
+    }
+  }
+}
+
 // Flat product loop for group rows.  A entries are taken G at a time: lane j
 // loads entry j's column, value and B row bounds, so a chunk's loads are all
 // in flight together; a group scan of the B row lengths numbers the chunk's
 // products and lanes take products lane, lane + G, ... (U per step, loads in
 // flight), each finding its entry as the last one whose first product number
-// is <= its own.  G = 32 keeps the per-entry data in registers (shuffles);
+// is <= its own.  G = 32 keeps the per-entry data in registers (warp_chunk);
 // larger groups stage it in `stage` (24 bytes per lane of shared memory).
 template <int G, bool NUM, typename PT, typename VT, typename F>
 __device__ __forceinline__ void for_products_flat(
@@ -136,61 +183,43 @@ __device__ __forceinline__ void for_products_flat(
       b0 = IX(__ldg(Bp + k));
       len = IX(__ldg(Bp + k + 1)) - b0;
     }
-    IX tot;
-    IX pre;
     if constexpr (G == 32) {
-      const IX inc = warp_scan_incl(len);
-      tot = __shfl_sync(0xffffffffu, inc, 31);
-      pre = inc - len;
+      warp_chunk<NUM, IX, VT>(Bj, Bx, b0, len, a, nc, lane, fn);
+      continue;  // no staging to guard
     } else {
-      pre = group_excl_scan<G, int64_t>(len, tmp, gid, &tot);
-    }
-    if constexpr (G != 32) {
+      IX tot;
+      const IX pre = group_excl_scan<G, int64_t>(len, tmp, gid, &tot);
       if (lane < nc) {
         spre[lane] = pre;
         sb0[lane] = b0;
         sa[lane] = a;
       }
       group_sync<G>(gid);
-    }
-    // the step loop is uniform across the group (the G = 32 search shuffles)
-    for (IX pb = 0; pb < tot; pb += IX(G) * U) {
-      int32_t cc[U];
-      VT xv[U], av[U];
+      // the step loop is uniform across the group
+      for (IX pb = 0; pb < tot; pb += IX(G) * U) {
+        int32_t cc[U];
+        VT xv[U], av[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const IX p = pb + IX(u) * G + lane;
-        int j = 0;
-        IX pj, bj;
-        if constexpr (G == 32) {
-#pragma unroll
-          for (int st = 16; st > 0; st >>= 1) {
-            const IX v = __shfl_sync(0xffffffffu, pre, (j + st) & 31);
-            if (j + st < nc && v <= p) j += st;
-          }
-          pj = __shfl_sync(0xffffffffu, pre, j);
-          bj = __shfl_sync(0xffffffffu, b0, j);
-          if constexpr (NUM) av[u] = __shfl_sync(0xffffffffu, a, j);
-        } else {
+        for (int u = 0; u < U; ++u) {
+          const IX p = pb + IX(u) * G + lane;
+          int j = 0;
           for (int st = G / 2; st > 0; st >>= 1)
             if (j + st < nc && spre[j + st] <= p) j += st;
-          pj = spre[j];
-          bj = sb0[j];
+          const IX q = IX(sb0[j]) + (p - IX(spre[j]));
           if constexpr (NUM) av[u] = sa[j];
+          cc[u] = p < tot ? __ldg(Bj + q) : -1;
+          if constexpr (NUM) xv[u] = p < tot ? __ldg(Bx + q) : VT(0);
         }
-        const IX q = bj + (p - pj);
-        cc[u] = p < tot ? __ldg(Bj + q) : -1;
-        if constexpr (NUM) xv[u] = p < tot ? __ldg(Bx + q) : VT(0);
-      }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (cc[u] >= 0) {
-          if constexpr (NUM) fn(cc[u], av[u] * xv[u]);
-          else fn(cc[u], VT(0));
+        for (int u = 0; u < U; ++u) {
+          if (cc[u] >= 0) {
+            if constexpr (NUM) fn(cc[u], av[u] * xv[u]);
+            else fn(cc[u], VT(0));
+          }
         }
       }
+      group_sync<G>(gid);  // the next chunk reuses the staging
     }
-    group_sync<G>(gid);  // the next chunk reuses the staging
   }
 }
 
@@ -396,7 +425,11 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for_addend<false>(P, m.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
-  const int64_t total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
+  int64_t total;
+  if constexpr (G == 32)
+    total = int64_t(__reduce_add_sync(0xffffffffu, unsigned(cnt)));  // cnt <= T <= 2^15
+  else
+    total = group_sum<G, int64_t>(int64_t(cnt), gm.tmp, gid);
   if (lane == 0) A.rowc[m.g] = int32_t(total);
   group_sync<G>(gid);
   prof_sub_g(A, 11, tp, lane == 0);
@@ -554,6 +587,52 @@ __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
   return src;
 }
 
+// Output of a warp row whose table has at most 64 slots (so c <= 32): slot
+// s = lane + 32 h is compacted by ballots into a list of the row's columns
+// behind the table (keys + 64), and every column's output position is its
+// rank in that list (the columns are distinct), counted with broadcast reads;
+// no sort.  With CS > 0 the values are spread over NC copies CS apart.
+template <int NC, typename PT, typename VT>
+__device__ __forceinline__ void warp_lean_output(const ProdDev<PT, VT> &P, const PhaseArgs &A,
+                                                 int *keys, const VT *vals, uint32_t T,
+                                                 uint32_t CS, int64_t c, int64_t off, int lane) {
+  const unsigned lt = (1u << lane) - 1u;
+  const int k0 = keys[lane];
+  const int k1 = T > 32 ? keys[lane + 32] : -1;
+  VT v0 = vals[lane];
+  VT v1 = T > 32 ? vals[lane + 32] : VT(0);
+  if (CS > 0) {
+#pragma unroll
+    for (int k = 1; k < NC; ++k) {
+      v0 += vals[k * CS + lane];
+      if (T > 32) v1 += vals[k * CS + lane + 32];
+    }
+  }
+  const unsigned m0 = __ballot_sync(0xffffffffu, k0 != -1);
+  const unsigned m1 = __ballot_sync(0xffffffffu, k1 != -1);
+  const int n0 = __popc(m0), nt = n0 + __popc(m1);
+  int *lk = keys + 64;  // behind the table (the key array has >= 128 slots)
+  if (k0 != -1) lk[__popc(m0 & lt)] = k0;
+  if (k1 != -1) lk[n0 + __popc(m1 & lt)] = k1;
+  __syncwarp();
+  int r0 = 0, r1 = 0;
+  for (int j = 0; j < nt; ++j) {
+    const int kj = lk[j];
+    r0 += kj < k0;
+    r1 += kj < k1;
+  }
+  if (lane == 0 && nt != c) set_error(A.err, 103);
+  if (k0 != -1 && r0 < c) {
+    P.Cj[off + r0] = k0;
+    P.Cx[off + r0] = v0;
+  }
+  if (k1 != -1 && r1 < c) {
+    P.Cj[off + r1] = k1;
+    P.Cx[off + r1] = v1;
+  }
+  __syncwarp();  // the next row clears the table
+}
+
 template <int G, int TMAX, typename PT, typename VT>
 __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                              const RowMeta &m, unsigned char *slice, const GroupMem &gm,
@@ -573,14 +652,24 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   if (T > TMAX) T = TMAX;
   const int logT = ilog2_pow2(T);
   const uint32_t mask = T - 1;
+  // Warp rows of at most 64 slots spread their values over NC copies of the
+  // value table (lane & (NC - 1) picks one; copies 16 bytes apart in banks):
+  // the FP64 shared atomics of lanes that hit one column in one step contend
+  // (products of neighbouring B rows share columns: Galerkin A·P numeric
+  // phase 3.72 ms with one table, 3.45 ms with 4 copies).
+  constexpr int NC = G == 32 ? 4 : 1;
+  static_assert(NC * (64 + 4) * 8 <= TMAX * 8, "value copies");
+  const bool copies = NC > 1 && T <= 64;
+  const uint32_t CS = T + 16 / uint32_t(sizeof(VT));  // copy stride
   clear_keys<G>(keys, T, lane);
-  clear_vals<G, VT>(vals, T, lane);
+  clear_vals<G, VT>(vals, copies ? NC * CS : T, lane);
   group_sync<G>(gid);
   const int64_t a0 = m.a0, a1 = m.a1;
   prof_sub_g(A, 9, tp, lane == 0);
+  VT *myv = copies ? vals + (lane & (NC - 1)) * CS : vals;
   auto ins = [&](int32_t col, VT v) {
     const uint32_t h = num_insert(keys, col, logT, mask, A.err);
-    atomicAdd(vals + h, v);
+    atomicAdd(myv + h, v);
   };
   if constexpr (G <= 256) {
     for_products_flat<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
@@ -593,6 +682,13 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for_addend<true>(P, m.r, lane, G, ins);
   group_sync<G>(gid);
   prof_sub_g(A, 10, tp, lane == 0);
+  if constexpr (G == 32) {
+    if (T <= 64) {
+      warp_lean_output<NC>(P, A, keys, vals, T, copies ? CS : 0, c, off, lane);
+      prof_sub_g(A, 13, tp, lane == 0);
+      return;
+    }
+  }
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
   // so first-half slots are held in registers across the group barrier inside
   // group_minmax; second-half slots are never overwritten.
