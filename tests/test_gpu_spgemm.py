@@ -151,6 +151,31 @@ def test_count_pass(ctx):
     assert upper == int(np.minimum(rm, A.ncols).sum())
 
 
+@pytest.mark.parametrize("bits", [32, 64])
+def test_count_pass_row_lengths(ctx, bits):
+    # The count pass walks rows of at most 64 A entries with one lane and
+    # longer ones with the whole warp, 32 rows per warp: rows of 0, 1, 63, 64,
+    # 65 and 700 entries side by side in one 32-row tile, the tile boundary
+    # crossed, and the product against the oracle (per-row products, totals,
+    # the product itself)
+    from trident_b200 import panels
+    rng = np.random.default_rng(17)
+    lens = [0, 64, 65, 63, 1, 700, 0, 64] * 5 + [65] * 7
+    n = 2000
+    rp = np.zeros(len(lens) + 1, dtype=np.int64)
+    rp[1:] = np.cumsum(lens)
+    col = np.concatenate([np.sort(rng.choice(n, size=k, replace=False)) for k in lens]).astype(np.int32)
+    A = HostCSR(len(lens), n, rp, col, rng.uniform(-1, 1, size=col.size))
+    B = random_csr(n, 300, density=0.02, seed=18)
+    dA, dB = A.to_device(rowptr_bits=bits), B.to_device(rowptr_bits=bits)
+    rm = oracle.row_mults(A, B)
+    np.testing.assert_array_equal(panels.row_products(ctx, dA, dB).cpu().numpy(), rm)
+    mults, upper = ops.spgemm_count(ctx, dA, dB)
+    assert mults == int(rm.sum())
+    assert upper == int(np.minimum(rm, B.ncols).sum())
+    check_product(ops.spgemm(ctx, dA, dB), A, B)
+
+
 def test_shape_mismatch_rejected(ctx):
     A = random_csr(4, 5, density=0.5, seed=1).to_device()
     B = random_csr(6, 7, density=0.5, seed=2).to_device()
