@@ -49,8 +49,12 @@ def parse():
     p.add_argument("--workload", default="rmat",
                    choices=["rmat", "uniform", "batched", "rap", "served", "summa", "coo"])
     p.add_argument("--rate", type=float, default=2000.0)
-    p.add_argument("--lanes", type=int, default=3, help="server worker lanes (served)")
-    p.add_argument("--max-batch", type=int, default=64, help="requests per server batch (served)")
+    # one lane: the lanes' persistent kernels take the whole GPU in turn, so
+    # more lanes only split the queue into smaller batches (served, 2000 req/s
+    # offered: 515 req/s with 1 lane, 462 with 2 or 3; at 80 % of the loop's
+    # rate p50 48 ms with 1 lane, 0.6 s with 2, 2.1 s with 3, one run each)
+    p.add_argument("--lanes", type=int, default=1, help="server worker lanes (served)")
+    p.add_argument("--max-batch", type=int, default=128, help="requests per server batch (served)")
     p.add_argument("--duration", type=float, default=5.0)
     p.add_argument("--products", type=int, default=512)
     p.add_argument("--scale", type=int, default=20)

@@ -221,7 +221,15 @@ int tspg_spgemm_row_products(tspg_ctx *ctx, void *stream, const tspg_csr *A,
  * how a row panel of one product is computed on its own GPU.
  * Empty operands give an empty C with a zeroed rowptr (the num_prods == 0
  * exit, include/cusparse_helpers.cuh:1251-1257).  Synchronises `stream` once
- * (to learn nnz(C)). */
+ * (to learn nnz(C)); twice when A has at least 65,536 rows.  Such a product
+ * whose rows are mostly warp rows (small product bounds) computes those rows
+ * whole in its first launch, into a workspace of 4 + val_bits / 8 bytes per
+ * unit of their output bound (at most 2^30 units) taken from the context's
+ * pool, and copies them into C in the second; when the budget refuses that
+ * workspace, or the product has few such rows, every row takes the two-pass
+ * path.  Results are the same either way; a plan (tspg_spgemm_symbolic)
+ * always takes the two-pass path, since its numeric calls may bring new
+ * values. */
 int tspg_spgemm(tspg_ctx *ctx, void *stream, const tspg_csr *A,
                 const tspg_csr *B, tspg_csr_out *C, int flags);
 

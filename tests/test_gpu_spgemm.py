@@ -176,6 +176,72 @@ def test_count_pass_row_lengths(ctx, bits):
     check_product(ops.spgemm(ctx, dA, dB), A, B)
 
 
+def _launches(ctx):
+    import ctypes as C
+
+    from trident_b200._lib import lib
+    n = C.c_int64()
+    lib.tspg_ctx_stats(ctx.h, C.byref(n))
+    return n.value
+
+
+@pytest.mark.parametrize("bits,vbits", [(32, 64), (64, 64), (32, 32)])
+def test_onepass_warp_rows(ctx, bits, vbits):
+    # A one-shot product of at least 65536 rows multiplies its warp rows whole
+    # in the symbolic launch (into a scratch), and the numeric launch copies
+    # them into C: Galerkin A·P on 42^3 (74,088 rows of ~119 products) into
+    # poisoned outputs, against the oracle.  The launch counts show the
+    # one-pass kernels ran: the one-shot call has 3 scan launches, the
+    # one-pass kernel and the copy more than a plan's symbolic + numeric
+    # calls, which have one operand-setting launch more
+    R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
+    assert A.nrows >= 1 << 16
+    dA, dP = A.to_device(rowptr_bits=bits, val_bits=vbits), P.to_device(rowptr_bits=bits, val_bits=vbits)
+    n0 = _launches(ctx)
+    ops.spgemm(ctx, dA, dP)
+    n1 = _launches(ctx)
+    plan = ops.Plan(ctx, dA, dP)
+    plan.numeric(dA, dP)
+    plan.close()
+    n2 = _launches(ctx)
+    assert (n1 - n0) - (n2 - n1) == 4
+    C1 = spgemm_poisoned(ctx, dA, dP)
+    r32 = (lambda M: HostCSR(M.nrows, M.ncols, M.rowptr, M.col, M.val.astype(np.float32).astype(np.float64)))
+    if vbits == 32:
+        check_product(C1, r32(A), r32(P), tol=TOL32)
+    else:
+        check_product(C1, A, P)
+
+
+def _vstack(*Ms):
+    rp = [np.zeros(1, np.int64)]
+    for M in Ms:
+        rp.append(M.rowptr[1:].astype(np.int64) + rp[-1][-1])
+    return HostCSR(sum(M.nrows for M in Ms), Ms[0].ncols, np.concatenate(rp),
+                   np.concatenate([M.col for M in Ms]), np.concatenate([M.val for M in Ms]))
+
+
+def test_onepass_mixed_row_classes(ctx):
+    # Most rows one-pass (Galerkin A·P on 42^3, ~12 columns each) beside rows
+    # whose first, 64-slot attempt is refused (40 random entries: ~150
+    # columns; redone with the full table) and rows of the 128-, 256- and
+    # CTA-thread classes (300 and 700 entries), into poisoned outputs
+    R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
+    rows = [A, random_csr(1500, A.ncols, per_row=40, seed=41), random_csr(300, A.ncols, per_row=300, seed=42),
+            random_csr(100, A.ncols, per_row=700, seed=43), random_csr(500, A.ncols, per_row=2, seed=44)]
+    Am = _vstack(*rows)
+    check_product(spgemm_poisoned(ctx, Am.to_device(), P.to_device()), Am, P)
+
+
+def test_onepass_without_eligible_rows(ctx):
+    # 70,000 rows of 600 products each (above the warp-row bound of the
+    # symbolic phase): no one-pass row, so the count pass runs again with
+    # every row two-pass
+    A = random_csr(70000, 2000, per_row=30, seed=31)
+    B = random_csr(2000, 1000, per_row=20, seed=32)
+    check_product(spgemm_poisoned(ctx, A.to_device(), B.to_device()), A, B)
+
+
 def test_shape_mismatch_rejected(ctx):
     A = random_csr(4, 5, density=0.5, seed=1).to_device()
     B = random_csr(6, 7, density=0.5, seed=2).to_device()

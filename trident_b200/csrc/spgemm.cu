@@ -36,7 +36,11 @@ static int set_smem_attr(int device) {
     cudaError_t e4 = cudaFuncSetAttribute(k_groups<PT, VT, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kGroupDynSmem);
-    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
+    cudaError_t e5 = cudaFuncSetAttribute(k_onepass<PT, VT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kGroupDynSmem);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess ||
+        e5 != cudaSuccess)
       return TSPG_ECUDA;
     if (cached) done[device] = true;
   }
@@ -69,6 +73,9 @@ struct tspg_plan {
   int64_t cur_stride = 0;
   int64_t *wide_a = nullptr, *wide_b = nullptr;  // widened row offsets (mixed widths)
   tspg_csr E{};        // addend of C = E + A·B (tspg_spgemm_acc), E.col == nullptr if none
+  int64_t onepass = 0;  // entries of the one-pass rows' scratch (0: none)
+  int32_t *oj = nullptr;
+  void *ox = nullptr;
   void *blocks[16];
   int nblocks = 0;
 
@@ -89,6 +96,16 @@ struct tspg_plan {
 };
 
 namespace tspg {
+
+// Internal flag of the one-shot product (tspg_spgemm): warp rows may be
+// multiplied whole in the symbolic launch (one-pass rows).  A plan that is
+// kept for numeric calls with new values cannot use it.
+constexpr int kFlagOnePass = 1 << 30;
+// ... and only on products of at least this many rows (it adds a scan and a
+// host round trip before the symbolic launch), with a scratch of at most
+// this many entries.
+constexpr int64_t kOnePassMinRows = 1 << 16;
+constexpr int64_t kOnePassMaxEntries = int64_t(1) << 30;
 
 static inline unsigned grid_for(int64_t work, int per_block, int cap) {
   int64_t g = (work + per_block - 1) / per_block;
@@ -118,8 +135,9 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   TSPG_TRY(P->get(&P->list, m));
   TSPG_TRY(P->get(&P->sched, 2));
   TSPG_TRY(P->get(&P->partial, P->nb + 1));
+  bool onepass = (flags & kFlagOnePass) && !(P->E.col && P->E.nnz > 0) && m >= kOnePassMinRows;
   TSPG_CUDA(ctx, cudaMemsetAsync(P->sched, 0, 2 * sizeof(Sched), s));
-  k_set_tune<<<1, 32, 0, s>>>(P->sched, 2, ctx->tune);
+  k_set_tune<<<1, 32, 0, s>>>(P->sched, 2, ctx->tune, onepass ? 1 : 0);
   TSPG_CUDA(ctx, cudaMemsetAsync(P->rowc, 0, (m > 0 ? m : 1) * sizeof(int32_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(P->cp, 0, sizeof(int64_t), s));
 
@@ -145,17 +163,50 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
     k_check_sorted_rows<PT><<<grid_for(B->nrows * 32, 256, ctx->num_sms * 16), 256,
                               0, s>>>(v.Bp, v.Bj, B->nrows, &prods->b_sorted);
   }
+  int extra = 0;
   if (m > 0) {
     k_row_mults<PT, VT><<<grid_for(m * 32, 256, ctx->num_sms * 16), 256, 0, s>>>(
-        prods, P->base, 1, m, P->rowf, P->sched);
+        prods, P->base, 1, m, P->rowf, P->sched, onepass ? P->rowc : nullptr);
+    if (onepass) {
+      // the one-pass rows' scratch offsets: a scan of their output bounds
+      k_scan_reduce<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial);
+      k_scan_partials<<<1, 1024, 0, s>>>(P->partial, P->nb);
+      k_scan_final<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial, P->nb,
+                                                            P->cp, P->sched + 1, nullptr);
+      extra += 3;
+      int64_t *h = ctx->h_words;
+      TSPG_CUDA(ctx, cudaMemcpyAsync(h, P->cp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      TSPG_CUDA(ctx, cudaMemcpyAsync(h + 1, &P->sched[0].cnt[CLS_ONEPASS], sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, s));
+      TSPG_CUDA(ctx, cudaStreamSynchronize(s));
+      const int64_t tot = h[0], rows = h[1];
+      // one pass when most rows take it (R-MAT 20: a tenth of the rows, and
+      // those with more than 32 outputs need their second attempt: +0.9 ms
+      // of symbolic phase; Galerkin A·P: every row, -0.9 ms per call)
+      if (tot > 0 && 2 * rows >= m && tot <= kOnePassMaxEntries &&
+          P->get(&P->oj, size_t(tot)) == TSPG_OK && P->get((VT **)&P->ox, size_t(tot)) == TSPG_OK) {
+        P->onepass = tot;
+      } else {  // every row two-pass: the one-pass rows back to the warp class
+        onepass = false;
+        k_fold_onepass<<<1, 32, 0, s>>>(P->sched);
+        TSPG_CUDA(ctx, cudaMemsetAsync(P->rowc, 0, m * sizeof(int32_t), s));
+        extra += 1;
+      }
+    }
     k_sched_offsets<<<1, 32, 0, s>>>(P->sched);
     k_scatter<PT, VT, 0><<<grid_for(m, 256, INT32_MAX), 256, 0, s>>>(
         prods, P->base, 1, m, P->rowf, P->rowc, P->cp, P->sched, P->list);
     PhaseArgs pa{P->base, P->sched, P->list, P->rowf, P->rowc, P->cp,
                  nullptr, 0, ctx->d_words + kErrWord, ctx->d_prof};
+    pa.oj = P->oj;
+    pa.ox = P->ox;
     phase_mark(ctx, 0, 0, s);
     k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
     k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
+    if (onepass) {
+      k_onepass<PT, VT><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
+      extra += 1;
+    }
     phase_mark(ctx, 0, 1, s);
     k_scan_reduce<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial);
     k_scan_partials<<<1, 1024, 0, s>>>(P->partial, P->nb);
@@ -163,7 +214,8 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                                                           P->nb, P->cp, P->sched + 1, P->rowf);
   }
   TSPG_CUDA(ctx, cudaGetLastError());
-  ctx->launches += 2 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 8 : 0);
+  ctx->launches += 2 + (!(flags & TSPG_F_B_SORTED) && B->nnz > 0 && B->nrows > 0) + (m > 0 ? 8 : 0) +
+                   extra;
   int64_t *h = ctx->h_words;
   TSPG_CUDA(ctx, cudaMemcpyAsync(h, P->cp + m, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   TSPG_CUDA(ctx, cudaMemcpyAsync(h + 1, &P->sched[0].total, 4 * sizeof(int64_t),
@@ -208,8 +260,11 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
   TSPG_CUDA(ctx, launch_dense_cluster<PT, VT>(ctx, s, prods, pa));
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
   k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
+  if (P->onepass)
+    k_onepass_copy<PT, VT><<<grid_for(m * 32, 256, ctx->num_sms * 16), 256, 0, s>>>(
+        prods, P->rowf, P->rowc, P->cp, P->oj, (const VT *)P->ox, m);
   phase_mark(ctx, 1, 1, s);
-  ctx->launches += 5;
+  ctx->launches += 5 + (P->onepass ? 1 : 0);
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
 }
@@ -376,7 +431,8 @@ extern "C" int tspg_spgemm(tspg_ctx *ctx, void *stream, const tspg_csr *A,
   TSPG_TRY(check_out(C, A->nrows, B->ncols, A->val_bits));
   tspg_plan *plan = nullptr;
   int64_t nnz = 0;
-  TSPG_TRY(tspg_spgemm_symbolic(ctx, stream, A, B, flags, &plan, &nnz));
+  TSPG_TRY(symbolic_entry(ctx, stream, A, B, nullptr, (flags & ~kFlagOnePass) | kFlagOnePass, &plan,
+                          &nnz));
   int st = TSPG_OK;
   if (C->rowptr_bits == 32 && nnz > INT32_MAX) st = TSPG_EOVERFLOW;
   if (st == TSPG_OK) st = ensure_out(C, nnz, A->val_bits / 8, (cudaStream_t)stream);

@@ -46,7 +46,7 @@ constexpr int kGroupDynSmem = kTableSmem + kGroupCountSmem;
 // Row classes, heaviest first.  The first four are worked by the whole CTA
 // (items fetched by one thread); G256 / G128 / G32 rows are fetched by each
 // group on its own, so groups never wait for one another.
-constexpr int NCLS = 7;
+constexpr int NCLS = 8;
 enum {
   CLS_DENSE0 = 0,  // DENSE rows with >= 2^20 products
   CLS_DENSE1 = 1,  // DENSE rows with >= 2^17 products
@@ -54,7 +54,8 @@ enum {
   CLS_G1024 = 3,
   CLS_G256 = 4,
   CLS_G128 = 5,
-  CLS_G32 = 6
+  CLS_G32 = 6,
+  CLS_ONEPASS = 7  // symbolic only: warp rows computed whole in the symbolic launch
 };
 constexpr int kCtaClasses = 4;  // classes [0, 4) are CTA-level
 __host__ __device__ constexpr bool cls_dense(int c) { return c <= CLS_DENSE2; }
@@ -88,8 +89,16 @@ __host__ __device__ inline int sym_class(int64_t f, int64_t n, const Tune &t) {
   if (fe <= t.sym[3]) return CLS_G1024;
   return dense_sub(f);
 }
+// One-pass warp rows (plain products only, Sched::onepass set): symbolic warp
+// rows whose table, sized by the product bound, fits a warp's numeric table
+// are multiplied in full in the symbolic launch; their output waits in a
+// scratch buffer for the numeric launch, which copies it into C.
+__host__ __device__ inline bool onepass_row(int64_t f, int64_t n, const Tune &t) {
+  const int64_t fe = f < n ? f : n;
+  return f > 0 && fe <= t.sym[0] && int64_t(t.load) * fe <= kNumT32;
+}
 __host__ __device__ inline int num_class(int64_t c, int64_t f, const Tune &t) {
-  if (c == 0) return -1;
+  if (c == 0 || f < 0) return -1;  // f < 0: a one-pass row, already computed
   if (c <= t.num[0]) return CLS_G32;
   if (c <= t.num[1]) return CLS_G128;
   if (c <= t.num[2]) return CLS_G256;
@@ -146,6 +155,8 @@ struct Sched {
   int64_t max_a_row;  // longest A row (sizes the DENSE cursor scratch)
   int64_t nonempty;
   unsigned long long work2;  // row counter of the cluster kernel (column-window rows)
+  int32_t onepass;  // symbolic record of a plain product: one-pass warp rows on
+  int32_t pad32;
   int64_t pad[2];
 };
 
@@ -184,8 +195,11 @@ __device__ __forceinline__ int subgroup_width_avg(int64_t f, int64_t na, int G) 
 // Setup kernels
 
 // Row binning of a run into its Sched records (after they were zeroed).
-static __global__ void k_set_tune(Sched *S, int n, Tune t) {
-  if (threadIdx.x < n) S[threadIdx.x].tune = t;
+static __global__ void k_set_tune(Sched *S, int n, Tune t, int onepass = 0) {
+  if (threadIdx.x < n) {
+    S[threadIdx.x].tune = t;
+    S[threadIdx.x].onepass = threadIdx.x == 0 ? onepass : 0;
+  }
 }
 
 template <typename PT, typename VT>
@@ -263,7 +277,7 @@ constexpr int kThreadRowMax = 64;
 template <typename PT, typename VT>
 __global__ void __launch_bounds__(256) k_row_mults(
     const ProdDev<PT, VT> *prods, const int64_t *base, int nprod, int64_t R,
-    int64_t *rowf, Sched *S) {
+    int64_t *rowf, Sched *S, int32_t *obound = nullptr) {
   __shared__ unsigned long long s_cnt[NCLS];
   __shared__ unsigned long long s_tot, s_up, s_ne;
   __shared__ long long s_maxa;
@@ -328,6 +342,10 @@ __global__ void __launch_bounds__(256) k_row_mults(
       rowf[g] = f;
       const int64_t n = prods[p].n;
       c = sym_class(f, n, S->tune);
+      // one-pass rows: their output bound min(f, n) sizes their scratch
+      const bool one = S->onepass && onepass_row(f, n, S->tune);
+      if (one) c = CLS_ONEPASS;
+      if (obound) obound[g] = one ? int32_t(f < n ? f : n) : 0;
       if (c >= 0) ne += 1;
       tot += f;
       up += f < n ? f : n;
@@ -366,6 +384,16 @@ __global__ void __launch_bounds__(256) k_row_mults(
   }
 }
 
+// The one-pass rows of a symbolic record go back to the warp class (the
+// product takes the two-pass path after all).
+static __global__ void k_fold_onepass(Sched *S) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    S->cnt[CLS_G32] += S->cnt[CLS_ONEPASS];
+    S->cnt[CLS_ONEPASS] = 0;
+    S->onepass = 0;
+  }
+}
+
 // Class offsets into the row list; resets the work counters.
 static __global__ void k_sched_offsets(Sched *S) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -401,6 +429,7 @@ __global__ void __launch_bounds__(256) k_scatter(
     r = g - base[p];
     if (MODE == 0) {
       c = sym_class(rowf[g], prods[p].n, S->tune);
+      if (S->onepass && onepass_row(rowf[g], prods[p].n, S->tune)) c = CLS_ONEPASS;
     } else {
       c = num_class(rowc[g], rowf[g], S->tune);
       const int64_t off = cp[g] - cp[base[p]];
@@ -516,7 +545,10 @@ static __global__ void __launch_bounds__(kScanThreads)
   for (int i = 0; i < kScanItems; ++i) {
     v[i] = (j0 + i < R) ? in[j0 + i] : 0;
     s += v[i];
-    if (rowf && v[i] > 0) packed += 1u << (4 * num_class(v[i], rowf[j0 + i], Snum->tune));
+    if (rowf && v[i] > 0) {
+      const int c = num_class(v[i], rowf[j0 + i], Snum->tune);
+      if (c >= 0) packed += 1u << (4 * c);
+    }
   }
   // class counts: a warp reduction per class, one shared atomic per warp
   // (rows of one class would otherwise all hit one counter)

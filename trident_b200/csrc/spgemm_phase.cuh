@@ -273,11 +273,39 @@ __device__ __forceinline__ uint32_t num_insert(int *keys, int32_t col,
   return 0;
 }
 
+// Insert for a table that admits at most about `cap` columns: ocnt[0] counts
+// the columns that took a slot, and once it reaches cap ocnt[1] is set and no
+// further column takes one (kRefused; the caller redoes the row with a full
+// table).  Columns already in the table are still found.  At most one column
+// per lane in flight gets in past the count, so a table of T = 2 cap slots
+// never fills (at most 2 cap - 1 columns) and every probe ends.
+constexpr uint32_t kRefused = 0xffffffffu;
+__device__ __forceinline__ uint32_t num_insert_capped(int *keys, int32_t col, int logT,
+                                                      uint32_t mask, int *ocnt, uint32_t cap) {
+  uint32_t h = hash_slot(col, logT);
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const int k = ((volatile int *)keys)[h];
+    if (k == col) return h;
+    if (k == -1) {
+      if (((volatile int *)ocnt)[1]) return kRefused;
+      const int old = atomicCAS(keys + h, -1, col);
+      if (old == -1) {
+        if (uint32_t(atomicAdd(ocnt, 1)) + 1 >= cap) ocnt[1] = 1;
+        return h;
+      }
+      if (old == col) return h;
+    }
+    h = (h + 1) & mask;
+  }
+  ocnt[1] = 1;  // not reached: the table never fills
+  return kRefused;
+}
+
 struct PhaseArgs {
   const int64_t *base;
   Sched *S;
   const uint64_t *list;
-  const int64_t *rowf;
+  int64_t *rowf;
   int32_t *rowc;
   const int64_t *cp;
   int32_t *curbuf;     // per-CTA cursor scratch for DENSE rows with long A rows:
@@ -285,6 +313,8 @@ struct PhaseArgs {
   int64_t cur_stride;  // entries per CTA in curbuf
   int64_t *err;
   unsigned long long *prof;  // optional: [class] cycles, [NCLS + class] rows
+  int32_t *oj = nullptr;     // one-pass rows: scratch columns and values
+  void *ox = nullptr;
 };
 
 // Optional per-class accounting (SM cycles spent in each row class), and
@@ -591,11 +621,14 @@ __device__ int radix_pairs(int *ka, VT *va, int *kb, VT *vb, int n, int bits,
 // s = lane + 32 h is compacted by ballots into a list of the row's columns
 // behind the table (keys + 64), and every column's output position is its
 // rank in that list (the columns are distinct), counted with broadcast reads;
-// no sort.  With CS > 0 the values are spread over NC copies CS apart.
-template <int NC, typename PT, typename VT>
-__device__ __forceinline__ void warp_lean_output(const ProdDev<PT, VT> &P, const PhaseArgs &A,
-                                                 int *keys, const VT *vals, uint32_t T,
-                                                 uint32_t CS, int64_t c, int64_t off, int lane) {
+// no sort.  With CS > 0 the values are spread over NC copies CS apart.  The
+// row goes to oj / ox; c is the count the symbolic phase found (checked), or
+// -1 when none did (one-pass rows).  Returns the row's count.
+template <int NC, typename VT>
+__device__ __forceinline__ int warp_lean_output(const PhaseArgs &A, int *keys, const VT *vals,
+                                                uint32_t T, uint32_t CS, int64_t c,
+                                                int32_t *__restrict__ oj, VT *__restrict__ ox,
+                                                int lane) {
   const unsigned lt = (1u << lane) - 1u;
   const int k0 = keys[lane];
   const int k1 = T > 32 ? keys[lane + 32] : -1;
@@ -621,19 +654,26 @@ __device__ __forceinline__ void warp_lean_output(const ProdDev<PT, VT> &P, const
     r0 += kj < k0;
     r1 += kj < k1;
   }
-  if (lane == 0 && nt != c) set_error(A.err, 103);
+  if (c < 0) c = nt;
+  else if (lane == 0 && nt != c) set_error(A.err, 103);
   if (k0 != -1 && r0 < c) {
-    P.Cj[off + r0] = k0;
-    P.Cx[off + r0] = v0;
+    oj[r0] = k0;
+    ox[r0] = v0;
   }
   if (k1 != -1 && r1 < c) {
-    P.Cj[off + r1] = k1;
-    P.Cx[off + r1] = v1;
+    oj[r1] = k1;
+    ox[r1] = v1;
   }
   __syncwarp();  // the next row clears the table
+  return nt;
 }
 
-template <int G, int TMAX, typename PT, typename VT>
+// ONEPASS (warp rows of a plain product, in the symbolic launch): m.c is the
+// row's output bound min(products, ncols) and m.off its scratch offset; the
+// row is written to the scratch (A.oj / A.ox) with the count found here, which
+// goes to rowc, and rowf becomes -1 - offset (the numeric launch copies the
+// row into C and skips it otherwise).
+template <int G, int TMAX, typename PT, typename VT, bool ONEPASS = false>
 __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                              const RowMeta &m, unsigned char *slice, const GroupMem &gm,
                              int gid, int lane) {
@@ -646,12 +686,12 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   int *keys = (int *)(slice + TMAX * 8);
   long long tp = clock64();
   const ProdDev<PT, VT> &P = prods[m.p];
-  const int64_t c = m.c;
+  int64_t c = m.c;  // one-pass rows: the bound until the compaction counts the row
   const int64_t off = m.off;
-  uint32_t T = pow2_at_least(A.S->tune.load * c, 32);
-  if (T > TMAX) T = TMAX;
-  const int logT = ilog2_pow2(T);
-  const uint32_t mask = T - 1;
+  int32_t *const oj = ONEPASS ? A.oj + off : P.Cj + off;
+  VT *const ox = ONEPASS ? (VT *)A.ox + off : P.Cx + off;
+  uint32_t Tfull = pow2_at_least(A.S->tune.load * c, 32);
+  if (Tfull > TMAX) Tfull = TMAX;
   // Warp rows of at most 64 slots spread their values over NC copies of the
   // value table (lane & (NC - 1) picks one; copies 16 bytes apart in banks):
   // the FP64 shared atomics of lanes that hit one column in one step contend
@@ -659,35 +699,71 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   // phase 3.72 ms with one table, 3.45 ms with 4 copies).
   constexpr int NC = G == 32 ? 4 : 1;
   static_assert(NC * (64 + 4) * 8 <= TMAX * 8, "value copies");
-  const bool copies = NC > 1 && T <= 64;
-  const uint32_t CS = T + 16 / uint32_t(sizeof(VT));  // copy stride
-  clear_keys<G>(keys, T, lane);
-  clear_vals<G, VT>(vals, copies ? NC * CS : T, lane);
-  group_sync<G>(gid);
+  // A one-pass row whose bound needs more than 64 slots first tries 64 (its
+  // count is unknown; the Galerkin A·P rows bound ~119 and hold ~12): once
+  // 32 columns are in (a counter in the warp's list slot) no new column gets
+  // a slot, and a refused column sends the row to a second attempt with the
+  // full table.
+  bool capped = ONEPASS && G == 32 && Tfull > 64;
+  int *ocnt = gm.lst;  // warp rows: [0] admitted columns, [1] refused
+  uint32_t T = Tfull;
+  int logT = 0;
+  uint32_t mask = 0;
   const int64_t a0 = m.a0, a1 = m.a1;
-  prof_sub_g(A, 9, tp, lane == 0);
-  VT *myv = copies ? vals + (lane & (NC - 1)) * CS : vals;
-  auto ins = [&](int32_t col, VT v) {
-    const uint32_t h = num_insert(keys, col, logT, mask, A.err);
-    atomicAdd(myv + h, v);
-  };
-  if constexpr (G <= 256) {
-    for_products_flat<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
-                                       gm.tmp, gm.stage, ins);
-  } else {
-    const int S = subgroup_width_avg(m.f, a1 - a0, G);
-    for_products_balanced<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, m.f, S, lane,
-                                           gid, gm.lst, gm.nl, gm.cap, ins);
-  }
-  for_addend<true>(P, m.r, lane, G, ins);
-  group_sync<G>(gid);
-  prof_sub_g(A, 10, tp, lane == 0);
-  if constexpr (G == 32) {
-    if (T <= 64) {
-      warp_lean_output<NC>(P, A, keys, vals, T, copies ? CS : 0, c, off, lane);
-      prof_sub_g(A, 13, tp, lane == 0);
-      return;
+  while (true) {
+    T = capped ? 64 : Tfull;
+    logT = ilog2_pow2(T);
+    mask = T - 1;
+    const bool copies = NC > 1 && T <= 64;
+    const uint32_t CS = T + 16 / uint32_t(sizeof(VT));  // copy stride
+    clear_keys<G>(keys, T, lane);
+    clear_vals<G, VT>(vals, copies ? NC * CS : T, lane);
+    if (capped && lane == 0) ocnt[0] = ocnt[1] = 0;
+    group_sync<G>(gid);
+    prof_sub_g(A, 9, tp, lane == 0);
+    VT *myv = copies ? vals + (lane & (NC - 1)) * CS : vals;
+    auto ins = [&](int32_t col, VT v) {
+      uint32_t h;
+      if (capped) {
+        h = num_insert_capped(keys, col, logT, mask, ocnt, T / 2);
+        if (h == kRefused) return;
+      } else {
+        h = num_insert(keys, col, logT, mask, A.err);
+      }
+      atomicAdd(myv + h, v);
+    };
+    if constexpr (G <= 256) {
+      for_products_flat<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, lane, gid,
+                                         gm.tmp, gm.stage, ins);
+    } else {
+      const int S = subgroup_width_avg(m.f, a1 - a0, G);
+      for_products_balanced<G, true, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1, m.f, S,
+                                             lane, gid, gm.lst, gm.nl, gm.cap, ins);
     }
+    for_addend<true>(P, m.r, lane, G, ins);
+    group_sync<G>(gid);
+    prof_sub_g(A, 10, tp, lane == 0);
+    if (capped) {
+      const bool refused = ((volatile int *)ocnt)[1] != 0;
+      __syncwarp();
+      if (refused) {  // more than 32 columns: again with the full table
+        capped = false;
+        continue;
+      }
+    }
+    if constexpr (G == 32) {
+      if (T <= 64) {
+        const int nt = warp_lean_output<NC>(A, keys, vals, T, copies ? CS : 0,
+                                            ONEPASS ? -1 : c, oj, ox, lane);
+        if (ONEPASS && lane == 0) {
+          A.rowc[m.g] = nt;
+          A.rowf[m.g] = -1 - off;
+        }
+        prof_sub_g(A, 13, tp, lane == 0);
+        return;
+      }
+    }
+    break;
   }
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
   // so first-half slots are held in registers across the group barrier inside
@@ -723,7 +799,12 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   int64_t tot;
   int64_t pos = group_excl_scan<G, int64_t>(int64_t(mine), tmp, gid, &tot);
   group_sync<G>(gid);
-  if (lane == 0 && tot != c) set_error(A.err, 103);
+  if (ONEPASS) c = tot;
+  else if (lane == 0 && tot != c) set_error(A.err, 103);
+  if (ONEPASS && lane == 0) {
+    A.rowc[m.g] = int32_t(c);
+    A.rowf[m.g] = -1 - off;
+  }
   const bool radix = c > kBitonicMax;
   const int bias = radix ? mn : 0;
 #pragma unroll
@@ -752,8 +833,8 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       warp_bitonic32<VT>(k, v, lane);
       prof_sub_g(A, 12, tp, lane == 0);
       if (lane < c) {
-        P.Cj[off + lane] = k;
-        P.Cx[off + lane] = v;
+        oj[lane] = k;
+        ox[lane] = v;
       }
       __syncwarp();
       prof_sub_g(A, 13, tp, lane == 0);
@@ -782,11 +863,9 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   prof_sub_g(A, 12, tp, lane == 0);
   const int *ko = src ? keys + H : keys;
   const VT *vo = src ? vals + H : vals;
-  int32_t *__restrict__ Cj = P.Cj + off;
-  VT *__restrict__ Cx = P.Cx + off;
   for (int64_t s = lane; s < c; s += G) {
-    Cj[s] = ko[s] + bias;
-    Cx[s] = vo[s];
+    oj[s] = ko[s] + bias;
+    ox[s] = vo[s];
   }
   group_sync<G>(gid);
   prof_sub_g(A, 13, tp, lane == 0);
@@ -1566,9 +1645,10 @@ __device__ __forceinline__ bool esc_fits(const RowMeta &m, int64_t fmax) {
 
 // Group-level rows of class `cls`: the group leader fetches one row index at a
 // time; the group exits when the class runs out.
-template <int G, bool NUM, typename PT, typename VT>
+template <int G, bool NUM, typename PT, typename VT, bool ONEPASS = false>
 __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                            int cls, unsigned char *smem, PhaseShared &sh) {
+  static_assert(!ONEPASS || (G == 32 && NUM), "one-pass rows are warp rows");
   constexpr int NG = kGroupThreads / G;  // groups of this size per CTA
   // slices start on 16-byte boundaries (the tables are cleared with 16-byte stores)
   constexpr int SLICE = (NUM ? kTableSmem / NG : (kTableSmem * 2 / 3) / NG) & ~15;
@@ -1620,7 +1700,9 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
       for (int t = 0; i < e; ++i, ++t) {
         const long long t0 = clock64();
         const RowMeta m = shfl_meta(mine, t);
-        if constexpr (NUM) {
+        if constexpr (ONEPASS) {
+          num_hash_row<G, TMAXN, PT, VT, true>(prods, A, m, slice, gm, gid, lane);
+        } else if constexpr (NUM) {
           if (esc_fits(m, TMAXN / 2))
             num_esc_row<G, TMAXN, PT, VT>(prods, A, m, slice, gm, gid, lane);
           else
@@ -1754,6 +1836,48 @@ __global__ void __launch_bounds__(kGroupThreads, 1)
   group_rows<256, NUM, PT, VT>(prods, A, CLS_G256, smem, sh);
   group_rows<128, NUM, PT, VT>(prods, A, CLS_G128, smem, sh);
   group_rows<32, NUM, PT, VT>(prods, A, CLS_G32, smem, sh);
+}
+
+// One-pass warp rows of a plain product (the symbolic record's CLS_ONEPASS
+// list), after k_groups in the symbolic launch: each row is multiplied in
+// full (the numeric warp-row form, its table sized by the output bound) into
+// the scratch.  A warp row's symbolic pass (hash count) is then not needed:
+// Galerkin A·P (27-point 128^3, ~119 products and ~12 outputs per row)
+// paid 1.8 ms of symbolic and 3.5 ms of numeric launches for it.
+template <typename PT, typename VT>
+__global__ void __launch_bounds__(kGroupThreads, 1)
+    k_onepass(const ProdDev<PT, VT> *prods, PhaseArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ PhaseShared sh;
+  if (threadIdx.x < NCLS) {
+    sh.off[threadIdx.x] = A.S->off[threadIdx.x];
+    sh.cnt[threadIdx.x] = A.S->cnt[threadIdx.x];
+  }
+  __syncthreads();
+  group_rows<32, true, PT, VT, true>(prods, A, CLS_ONEPASS, smem, sh);
+}
+
+// Numeric launch: the one-pass rows (rowf < 0) go from the scratch into C, a
+// warp per row.
+template <typename PT, typename VT>
+__global__ void __launch_bounds__(256) k_onepass_copy(const ProdDev<PT, VT> *prods,
+                                                      const int64_t *rowf, const int32_t *rowc,
+                                                      const int64_t *cp, const int32_t *oj,
+                                                      const VT *ox, int64_t R) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  int32_t *Cj = prods[0].Cj;
+  VT *Cx = prods[0].Cx;
+  for (int64_t g = warp; g < R; g += nwarps) {
+    const int64_t f = rowf[g];
+    if (f >= 0) continue;
+    const int64_t src = -1 - f, dst = cp[g], c = rowc[g];
+    for (int64_t q = lane; q < c; q += 32) {
+      Cj[dst + q] = oj[src + q];
+      Cx[dst + q] = ox[src + q];
+    }
+  }
 }
 
 }  // namespace tspg

@@ -156,12 +156,16 @@ class Plan:
 
 def spgemm(ctx: Context, A: DeviceCSR, B: DeviceCSR, rowptr_bits: int = 64, flags: int = 0,
            stream=None) -> DeviceCSR:
-    """C = A·B (LocalMatrix::spgemm, include/KokkosWrap.hpp:367-391)."""
-    p = Plan(ctx, A, B, flags, stream)
-    try:
-        return p.numeric(A, B, rowptr_bits, stream)
-    finally:
-        p.close()
+    """C = A·B (LocalMatrix::spgemm, include/KokkosWrap.hpp:367-391): one
+    tspg_spgemm call, its column and value arrays from the allocator hook once
+    nnz(C) is known (a plan kept for new values is `Plan`)."""
+    m, n = A.nrows, B.ncols
+    rp = torch.empty(m + 1, dtype=torch.int32 if rowptr_bits == 32 else torch.int64, device=A.rowptr.device)
+    alloc = _TorchAlloc(A.rowptr.device)
+    o = _out_struct(m, n, rp, A.val_bits, alloc=alloc)
+    a, b = A.abi(), B.abi()
+    check(lib.tspg_spgemm(ctx.h, _stream_ptr(stream), C.byref(a), C.byref(b), C.byref(o), flags), "tspg_spgemm")
+    return _finish(o, rp, alloc, A.val_bits)
 
 
 def spgemm_count(ctx: Context, A: DeviceCSR, B: DeviceCSR, stream=None):
