@@ -808,8 +808,16 @@ def run_served(args):
         (completed req/s, p50 ms, p99 ms, batches)."""
         n_req, kinds, picks, gaps = sequence(rate, duration, seed)
         srv = ops.Server(ctx, mem_budget=120 << 30, lanes=args.lanes, max_batch=args.max_batch)
-        # warm-up: one request of each kind
-        for t in (srv.submit(*ab_pool[0]), srv.submit(rap_pool[0][1], rap_pool[0][2], rap_pool[0][0])):
+        # warm-up: one full batch of the request mix (the lanes' batches map
+        # their output memory on the first admissions of that size)
+        warm = []
+        for i in range(min(n_req, args.max_batch * args.lanes)):
+            if kinds[i]:
+                warm.append(srv.submit(*ab_pool[picks[i]]))
+            else:
+                R, A, P = rap_pool[picks[i]]
+                warm.append(srv.submit(A, P, R))
+        for t in warm:
             srv.wait(t)
             srv.release(t)
         torch.cuda.synchronize()

@@ -233,6 +233,15 @@ def test_onepass_mixed_row_classes(ctx):
     check_product(spgemm_poisoned(ctx, Am.to_device(), P.to_device()), Am, P)
 
 
+def test_onepass_minority_folds_back(ctx):
+    # R-MAT 17 A·A (131,072 rows): a tenth of the rows qualify for the
+    # one-pass path, too few, so they go back to the warp class after their
+    # bounds were written (the count pass's bounds cleared again)
+    A = workloads.rmat(scale=17, edge_factor=16, seed=4)
+    dA = A.to_device()
+    check_product(spgemm_poisoned(ctx, dA, dA, flags=TSPG_F_B_SORTED), A, A)
+
+
 def test_onepass_without_eligible_rows(ctx):
     # 70,000 rows of 600 products each (above the warp-row bound of the
     # symbolic phase): no one-pass row, so the count pass runs again with

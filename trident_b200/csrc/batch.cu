@@ -387,7 +387,10 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
   // ---- output slab and graph 2: numeric
   bool regraph = rebuild;
   if (b->total_nnz > b->cap_nnz || !b->Cj) {
-    const int64_t nnz = b->total_nnz > 0 ? b->total_nnz : 1;
+    // grows by at least half its size, so a batch reused for larger and
+    // larger admissions (a server lane) maps new memory only a few times
+    const int64_t want = b->total_nnz > 0 ? b->total_nnz : 1;
+    const int64_t nnz = b->Cj && want < b->cap_nnz + b->cap_nnz / 2 ? b->cap_nnz + b->cap_nnz / 2 : want;
     TSPG_TRY(regrow(ctx, &b->Cj, nnz, s));
     TSPG_TRY(regrow(ctx, (VT **)&b->Cx, nnz, s));
     b->cap_nnz = nnz;
