@@ -192,8 +192,9 @@ def test_onepass_warp_rows(ctx, bits, vbits):
     # them into C: Galerkin A·P on 42^3 (74,088 rows of ~119 products) into
     # poisoned outputs, against the oracle.  The launch counts show the
     # one-pass kernels ran: the one-shot call has 3 scan launches, the
-    # one-pass kernel and the copy more than a plan's symbolic + numeric
-    # calls, which have one operand-setting launch more
+    # one-pass kernel, 3 launches for the rows sent back to the two-pass path
+    # and the copy more than a plan's symbolic + numeric calls, which have
+    # one operand-setting launch more
     R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
     assert A.nrows >= 1 << 16
     dA, dP = A.to_device(rowptr_bits=bits, val_bits=vbits), P.to_device(rowptr_bits=bits, val_bits=vbits)
@@ -204,7 +205,7 @@ def test_onepass_warp_rows(ctx, bits, vbits):
     plan.numeric(dA, dP)
     plan.close()
     n2 = _launches(ctx)
-    assert (n1 - n0) - (n2 - n1) == 4
+    assert (n1 - n0) - (n2 - n1) == 7
     C1 = spgemm_poisoned(ctx, dA, dP)
     r32 = (lambda M: HostCSR(M.nrows, M.ncols, M.rowptr, M.col, M.val.astype(np.float32).astype(np.float64)))
     if vbits == 32:
@@ -231,6 +232,26 @@ def test_onepass_mixed_row_classes(ctx):
             random_csr(100, A.ncols, per_row=700, seed=43), random_csr(500, A.ncols, per_row=2, seed=44)]
     Am = _vstack(*rows)
     check_product(spgemm_poisoned(ctx, Am.to_device(), P.to_device()), Am, P)
+
+
+def test_onepass_rows_sent_back(ctx):
+    # One-pass rows too large for a warp's full table (600 products each):
+    # those with fewer than 32 columns finish in their 64-slot attempt, the
+    # others (~500 columns) go back to the two-pass path within the same
+    # symbolic launch; 80,000 rows, half of each kind, into poisoned outputs
+    rng = np.random.default_rng(51)
+    rows_b, cols_b = [], []
+    for k in range(2000):
+        span = 24 if k < 1000 else 2000
+        rows_b.append(np.sort(rng.choice(span, size=20, replace=False)))
+    rpb = np.concatenate([[0], np.cumsum([len(r) for r in rows_b])]).astype(np.int64)
+    B = HostCSR(2000, 2000, rpb, np.concatenate(rows_b).astype(np.int32), rng.uniform(-1, 1, size=rpb[-1]))
+    rows_a = [np.sort(rng.choice(1000, size=30, replace=False)) + (0 if i % 2 == 0 else 1000) for i in range(80000)]
+    rpa = np.concatenate([[0], np.cumsum([30] * 80000)]).astype(np.int64)
+    A = HostCSR(80000, 2000, rpa, np.concatenate(rows_a).astype(np.int32), rng.uniform(-1, 1, size=rpa[-1]))
+    H = check_product(spgemm_poisoned(ctx, A.to_device(), B.to_device()), A, B)
+    c = np.diff(H.rowptr)
+    assert c[0::2].max() < 32 and c[1::2].min() >= 32
 
 
 def test_onepass_minority_folds_back(ctx):

@@ -66,7 +66,7 @@ struct tspg_plan {
   int32_t *rowc = nullptr;
   int64_t *cp = nullptr;
   uint64_t *list = nullptr;
-  Sched *sched = nullptr;  // [0] symbolic, [1] numeric
+  Sched *sched = nullptr;  // [0] symbolic, [1] numeric, [2] deferred one-pass rows
   int64_t *partial = nullptr;
   int64_t nb = 0;
   int32_t *curbuf = nullptr;
@@ -76,6 +76,7 @@ struct tspg_plan {
   int64_t onepass = 0;  // entries of the one-pass rows' scratch (0: none)
   int32_t *oj = nullptr;
   void *ox = nullptr;
+  uint64_t *defer = nullptr;
   void *blocks[16];
   int nblocks = 0;
 
@@ -133,11 +134,11 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
   TSPG_TRY(P->get(&P->rowc, m));
   TSPG_TRY(P->get(&P->cp, m + 1));
   TSPG_TRY(P->get(&P->list, m));
-  TSPG_TRY(P->get(&P->sched, 2));
+  TSPG_TRY(P->get(&P->sched, 3));
   TSPG_TRY(P->get(&P->partial, P->nb + 1));
   bool onepass = (flags & kFlagOnePass) && !(P->E.col && P->E.nnz > 0) && m >= kOnePassMinRows;
-  TSPG_CUDA(ctx, cudaMemsetAsync(P->sched, 0, 2 * sizeof(Sched), s));
-  k_set_tune<<<1, 32, 0, s>>>(P->sched, 2, ctx->tune, onepass ? 1 : 0);
+  TSPG_CUDA(ctx, cudaMemsetAsync(P->sched, 0, 3 * sizeof(Sched), s));
+  k_set_tune<<<1, 32, 0, s>>>(P->sched, 3, ctx->tune, onepass ? 1 : 0);
   TSPG_CUDA(ctx, cudaMemsetAsync(P->rowc, 0, (m > 0 ? m : 1) * sizeof(int32_t), s));
   TSPG_CUDA(ctx, cudaMemsetAsync(P->cp, 0, sizeof(int64_t), s));
 
@@ -184,9 +185,10 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
       // those with more than 32 outputs need their second attempt: +0.9 ms
       // of symbolic phase; Galerkin A·P: every row, -0.9 ms per call)
       if (tot > 0 && 2 * rows >= m && tot <= kOnePassMaxEntries &&
-          P->get(&P->oj, size_t(tot)) == TSPG_OK && P->get((VT **)&P->ox, size_t(tot)) == TSPG_OK) {
+          P->get(&P->oj, size_t(tot)) == TSPG_OK && P->get((VT **)&P->ox, size_t(tot)) == TSPG_OK &&
+          P->get(&P->defer, size_t(rows)) == TSPG_OK) {
         P->onepass = tot;
-      } else {  // every row two-pass: the one-pass rows back to the warp class
+      } else {  // every row two-pass: the one-pass rows back to their classes
         onepass = false;
         k_fold_onepass<<<1, 32, 0, s>>>(P->sched);
         TSPG_CUDA(ctx, cudaMemsetAsync(P->rowc, 0, m * sizeof(int32_t), s));
@@ -200,12 +202,23 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
                  nullptr, 0, ctx->d_words + kErrWord, ctx->d_prof};
     pa.oj = P->oj;
     pa.ox = P->ox;
+    pa.defer = P->defer;
     phase_mark(ctx, 0, 0, s);
     k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
     k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
     if (onepass) {
       k_onepass<PT, VT><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
-      extra += 1;
+      // the rows sent back (too many columns for their 64-slot attempt and
+      // too large for a warp's full table): their symbolic count, as
+      // 256-thread rows of their own record
+      Sched *D = P->sched + 2;
+      k_defer_setup<<<1, 32, 0, s>>>(P->sched, D);
+      k_sched_offsets<<<1, 32, 0, s>>>(D);
+      PhaseArgs pd = pa;
+      pd.S = D;
+      pd.list = P->defer;
+      k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pd);
+      extra += 4;
     }
     phase_mark(ctx, 0, 1, s);
     k_scan_reduce<<<(unsigned)P->nb, kScanThreads, 0, s>>>(P->rowc, m, P->partial);

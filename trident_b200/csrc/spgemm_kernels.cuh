@@ -89,13 +89,22 @@ __host__ __device__ inline int sym_class(int64_t f, int64_t n, const Tune &t) {
   if (fe <= t.sym[3]) return CLS_G1024;
   return dense_sub(f);
 }
-// One-pass warp rows (plain products only, Sched::onepass set): symbolic warp
-// rows whose table, sized by the product bound, fits a warp's numeric table
-// are multiplied in full in the symbolic launch; their output waits in a
-// scratch buffer for the numeric launch, which copies it into C.
+// One-pass rows (plain products only, Sched::onepass set): rows of the
+// symbolic warp, 128- and 256-thread classes are multiplied whole by a warp
+// in the symbolic launch; their output waits in a scratch buffer for the
+// numeric launch, which copies it into C.  A row whose output bound
+// min(f, n) fits a warp's numeric table is always finished there; a larger
+// one is finished only when it has fewer than kCappedCols columns (its
+// 64-slot attempt), else it is deferred to the two-pass path.
+constexpr int kCappedCols = 32;
 __host__ __device__ inline bool onepass_row(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
-  return f > 0 && fe <= t.sym[0] && int64_t(t.load) * fe <= kNumT32;
+  return f > 0 && fe <= t.sym[2];
+}
+// Scratch entries a one-pass row may write.
+__host__ __device__ inline int64_t onepass_bound(int64_t f, int64_t n, const Tune &t) {
+  const int64_t fe = f < n ? f : n;
+  return int64_t(t.load) * fe <= kNumT32 ? fe : kCappedCols;
 }
 __host__ __device__ inline int num_class(int64_t c, int64_t f, const Tune &t) {
   if (c == 0 || f < 0) return -1;  // f < 0: a one-pass row, already computed
@@ -155,8 +164,10 @@ struct Sched {
   int64_t max_a_row;  // longest A row (sizes the DENSE cursor scratch)
   int64_t nonempty;
   unsigned long long work2;  // row counter of the cluster kernel (column-window rows)
-  int32_t onepass;  // symbolic record of a plain product: one-pass warp rows on
+  int32_t onepass;  // symbolic record of a plain product: one-pass rows on
   int32_t pad32;
+  int64_t cand[NCLS];           // one-pass candidates by the class they left
+  unsigned long long ndefer;    // one-pass rows sent back to the two-pass path
   int64_t pad[2];
 };
 
@@ -278,10 +289,10 @@ template <typename PT, typename VT>
 __global__ void __launch_bounds__(256) k_row_mults(
     const ProdDev<PT, VT> *prods, const int64_t *base, int nprod, int64_t R,
     int64_t *rowf, Sched *S, int32_t *obound = nullptr) {
-  __shared__ unsigned long long s_cnt[NCLS];
+  __shared__ unsigned long long s_cnt[NCLS], s_cand[NCLS];
   __shared__ unsigned long long s_tot, s_up, s_ne;
   __shared__ long long s_maxa;
-  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = 0;
+  if (threadIdx.x < NCLS) s_cnt[threadIdx.x] = s_cand[threadIdx.x] = 0;
   if (threadIdx.x == 0) s_tot = s_up = s_ne = 0, s_maxa = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -332,7 +343,7 @@ __global__ void __launch_bounds__(256) k_row_mults(
       sum = warp_sum(sum);
       if (lane == j) f = sum;
     }
-    int c = -1;
+    int c = -1, left = -1;
     if (valid) {
       if (prods[p].Ej) {  // the addend's entries count as products of the row
         int64_t e0, e1;
@@ -342,10 +353,14 @@ __global__ void __launch_bounds__(256) k_row_mults(
       rowf[g] = f;
       const int64_t n = prods[p].n;
       c = sym_class(f, n, S->tune);
-      // one-pass rows: their output bound min(f, n) sizes their scratch
+      // one-pass rows: their scratch bound; the class they leave is kept
+      // (cand) in case the product takes the two-pass path after all
       const bool one = S->onepass && onepass_row(f, n, S->tune);
-      if (one) c = CLS_ONEPASS;
-      if (obound) obound[g] = one ? int32_t(f < n ? f : n) : 0;
+      if (one) {
+        left = c;
+        c = CLS_ONEPASS;
+      }
+      if (obound) obound[g] = one ? int32_t(onepass_bound(f, n, S->tune)) : 0;
       if (c >= 0) ne += 1;
       tot += f;
       up += f < n ? f : n;
@@ -356,6 +371,12 @@ __global__ void __launch_bounds__(256) k_row_mults(
       const int cl = __shfl_sync(0xffffffffu, c, __ffs(todo) - 1);
       const unsigned m = __ballot_sync(0xffffffffu, c == cl);
       if (lane == __ffs(m) - 1) atomicAdd(&s_cnt[cl], (unsigned long long)__popc(m));
+      todo &= ~m;
+    }
+    for (unsigned todo = __ballot_sync(0xffffffffu, left >= 0); todo;) {
+      const int cl = __shfl_sync(0xffffffffu, left, __ffs(todo) - 1);
+      const unsigned m = __ballot_sync(0xffffffffu, left == cl);
+      if (lane == __ffs(m) - 1) atomicAdd(&s_cand[cl], (unsigned long long)__popc(m));
       todo &= ~m;
     }
   }
@@ -376,6 +397,8 @@ __global__ void __launch_bounds__(256) k_row_mults(
   __syncthreads();
   if (threadIdx.x < NCLS && s_cnt[threadIdx.x])
     atomicAdd((unsigned long long *)&S->cnt[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x < NCLS && s_cand[threadIdx.x])
+    atomicAdd((unsigned long long *)&S->cand[threadIdx.x], s_cand[threadIdx.x]);
   if (threadIdx.x == 0) {
     atomicAdd((unsigned long long *)&S->total, s_tot);
     atomicAdd((unsigned long long *)&S->upper, s_up);
@@ -384,14 +407,20 @@ __global__ void __launch_bounds__(256) k_row_mults(
   }
 }
 
-// The one-pass rows of a symbolic record go back to the warp class (the
-// product takes the two-pass path after all).
+// The one-pass rows of a symbolic record go back to the classes they left
+// (the product takes the two-pass path after all).
 static __global__ void k_fold_onepass(Sched *S) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    S->cnt[CLS_G32] += S->cnt[CLS_ONEPASS];
+    for (int c = 0; c < NCLS; ++c) S->cnt[c] += S->cand[c];
     S->cnt[CLS_ONEPASS] = 0;
     S->onepass = 0;
   }
+}
+
+// The record of the one-pass rows sent back to the two-pass path (their
+// list: the deferred rows), counted as 256-thread symbolic rows.
+static __global__ void k_defer_setup(const Sched *S, Sched *D) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) D->cnt[CLS_G256] = int64_t(S->ndefer);
 }
 
 // Class offsets into the row list; resets the work counters.

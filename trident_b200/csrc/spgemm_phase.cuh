@@ -315,6 +315,7 @@ struct PhaseArgs {
   unsigned long long *prof;  // optional: [class] cycles, [NCLS + class] rows
   int32_t *oj = nullptr;     // one-pass rows: scratch columns and values
   void *ox = nullptr;
+  uint64_t *defer = nullptr;  // one-pass rows sent back to the two-pass path
 };
 
 // Optional per-class accounting (SM cycles spent in each row class), and
@@ -668,11 +669,14 @@ __device__ __forceinline__ int warp_lean_output(const PhaseArgs &A, int *keys, c
   return nt;
 }
 
-// ONEPASS (warp rows of a plain product, in the symbolic launch): m.c is the
-// row's output bound min(products, ncols) and m.off its scratch offset; the
-// row is written to the scratch (A.oj / A.ox) with the count found here, which
-// goes to rowc, and rowf becomes -1 - offset (the numeric launch copies the
-// row into C and skips it otherwise).
+// ONEPASS (rows of a plain product taken by a warp in the symbolic launch):
+// m.off is the row's scratch offset; the row is written to the scratch
+// (A.oj / A.ox) with the count found here, which goes to rowc, and rowf
+// becomes -1 - offset (the numeric launch copies the row into C and skips it
+// otherwise).  A row whose bound min(products, ncols) is too large for a
+// warp's full table and which holds kCappedCols columns or more is instead
+// listed in A.defer for the two-pass path (its symbolic count follows in the
+// same launch).
 template <int G, int TMAX, typename PT, typename VT, bool ONEPASS = false>
 __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                              const RowMeta &m, unsigned char *slice, const GroupMem &gm,
@@ -686,11 +690,13 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   int *keys = (int *)(slice + TMAX * 8);
   long long tp = clock64();
   const ProdDev<PT, VT> &P = prods[m.p];
-  int64_t c = m.c;  // one-pass rows: the bound until the compaction counts the row
+  // one-pass rows: the output bound until the compaction counts the row
+  int64_t c = ONEPASS ? (m.f < P.n ? m.f : P.n) : m.c;
   const int64_t off = m.off;
   int32_t *const oj = ONEPASS ? A.oj + off : P.Cj + off;
   VT *const ox = ONEPASS ? (VT *)A.ox + off : P.Cx + off;
   uint32_t Tfull = pow2_at_least(A.S->tune.load * c, 32);
+  const bool full_fits = Tfull <= TMAX;
   if (Tfull > TMAX) Tfull = TMAX;
   // Warp rows of at most 64 slots spread their values over NC copies of the
   // value table (lane & (NC - 1) picks one; copies 16 bytes apart in banks):
@@ -746,8 +752,16 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     if (capped) {
       const bool refused = ((volatile int *)ocnt)[1] != 0;
       __syncwarp();
-      if (refused) {  // more than 32 columns: again with the full table
-        capped = false;
+      if (refused) {
+        if (!full_fits) {  // too large for a warp: the two-pass path
+          if (lane == 0) {
+            const unsigned long long i = atomicAdd(&A.S->ndefer, 1ull);
+            A.defer[i] = (uint64_t(m.p) << 40) | uint64_t(m.r);
+          }
+          __syncwarp();
+          return;
+        }
+        capped = false;  // again with the full table
         continue;
       }
     }
