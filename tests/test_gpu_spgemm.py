@@ -235,15 +235,16 @@ def test_onepass_mixed_row_classes(ctx):
 
 
 def test_onepass_rows_sent_back(ctx):
-    # One-pass rows too large for a warp's full table (600 products each):
-    # those with fewer than 32 columns finish in their 64-slot attempt, the
-    # others (~500 columns) go back to the two-pass path within the same
-    # symbolic launch; 80,000 rows, half of each kind, into poisoned outputs
+    # One-pass rows too large for a warp's full table (600 products each,
+    # every B row starting on column 0, so all are candidates): those with
+    # fewer than 32 columns finish in their 64-slot attempt, the others
+    # (~500 columns) go back to the two-pass path within the same symbolic
+    # launch sequence; 80,000 rows, half of each kind, into poisoned outputs
     rng = np.random.default_rng(51)
-    rows_b, cols_b = [], []
+    rows_b = []
     for k in range(2000):
         span = 24 if k < 1000 else 2000
-        rows_b.append(np.sort(rng.choice(span, size=20, replace=False)))
+        rows_b.append(np.concatenate([[0], np.sort(rng.choice(np.arange(1, span), size=19, replace=False))]))
     rpb = np.concatenate([[0], np.cumsum([len(r) for r in rows_b])]).astype(np.int64)
     B = HostCSR(2000, 2000, rpb, np.concatenate(rows_b).astype(np.int32), rng.uniform(-1, 1, size=rpb[-1]))
     rows_a = [np.sort(rng.choice(1000, size=30, replace=False)) + (0 if i % 2 == 0 else 1000) for i in range(80000)]
@@ -252,6 +253,26 @@ def test_onepass_rows_sent_back(ctx):
     H = check_product(spgemm_poisoned(ctx, A.to_device(), B.to_device()), A, B)
     c = np.diff(H.rowptr)
     assert c[0::2].max() < 32 and c[1::2].min() >= 32
+
+
+def test_onepass_skips_rows_without_repeats(ctx):
+    # 80,000 uniform-random rows of 600 products (~590 columns): too large for
+    # a warp's full table, and their B rows do not start on shared columns,
+    # so they are no one-pass candidates and the product keeps the two-pass
+    # path (no launch beyond the count-pass scan and the fold)
+    A = random_csr(80000, 2000, per_row=30, seed=61)
+    B = random_csr(2000, 20000, per_row=20, seed=62)
+    dA, dB = A.to_device(), B.to_device()
+    n0 = _launches(ctx)
+    ops.spgemm(ctx, dA, dB)
+    n1 = _launches(ctx)
+    plan = ops.Plan(ctx, dA, dB)
+    plan.numeric(dA, dB)
+    plan.close()
+    n2 = _launches(ctx)
+    # 3 scan launches and the fold more; one operand-setting launch less
+    assert (n1 - n0) - (n2 - n1) == 3
+    check_product(spgemm_poisoned(ctx, dA, dB), A, B)
 
 
 def test_onepass_minority_folds_back(ctx):

@@ -101,10 +101,15 @@ __host__ __device__ inline bool onepass_row(int64_t f, int64_t n, const Tune &t)
   const int64_t fe = f < n ? f : n;
   return f > 0 && fe <= t.sym[2];
 }
-// Scratch entries a one-pass row may write.
+// A one-pass row whose full table fits a warp (else only its 64-slot attempt
+// can finish it), and the scratch entries it may write.
+__host__ __device__ inline bool onepass_full(int64_t f, int64_t n, const Tune &t) {
+  const int64_t fe = f < n ? f : n;
+  return int64_t(t.load) * fe <= kNumT32;
+}
 __host__ __device__ inline int64_t onepass_bound(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
-  return int64_t(t.load) * fe <= kNumT32 ? fe : kCappedCols;
+  return onepass_full(f, n, t) ? fe : kCappedCols;
 }
 __host__ __device__ inline int num_class(int64_t c, int64_t f, const Tune &t) {
   if (c == 0 || f < 0) return -1;  // f < 0: a one-pass row, already computed
@@ -275,6 +280,8 @@ __global__ void k_check_sorted_rows(const PT *Bp, const int32_t *Bj,
 // reduction), block-aggregated class counts.
 // Rows of at most this many A entries are walked by one lane in k_row_mults.
 constexpr int kThreadRowMax = 64;
+// A entries a one-pass candidate looks at for repeated columns.
+constexpr int kHintEntries = 8;
 
 // Products per row (rowf), the symbolic class counts, the product total, the
 // sum of min(products, ncols) and the longest A row.  A warp takes 32 rows at
@@ -343,6 +350,29 @@ __global__ void __launch_bounds__(256) k_row_mults(
       sum = warp_sum(sum);
       if (lane == j) f = sum;
     }
+    // One-pass candidates too large for a warp's full table also need their
+    // products to repeat columns: a row counts, over its first kHintEntries A
+    // entries, those whose B row starts on the same column as the previous
+    // entry's (0.5-0.6 of them on the Galerkin rows, 0.002 on uniform-random
+    // rows); a few loads per such row.
+    int same = 0, seen = 0;
+    {
+      const int64_t fe = f < (valid ? prods[p].n : 0) ? f : (valid ? prods[p].n : 0);
+      const bool need = S->onepass && valid && fe > 0 && fe <= S->tune.sym[2] &&
+                        int64_t(S->tune.load) * fe > kNumT32;
+      if (__any_sync(0xffffffffu, need)) {
+        const int32_t *Bj = valid ? prods[p].Bj : nullptr;
+        seen = need ? int(len < kHintEntries ? len : kHintEntries) : 0;
+        int prev = -2;
+        for (int t = 0; t < seen; ++t) {
+          const int64_t k = __ldg(Aj + a0 + t);
+          const int64_t q0 = int64_t(__ldg(Bp + k)), q1 = int64_t(__ldg(Bp + k + 1));
+          const int first = q1 > q0 ? __ldg(Bj + q0) : -1;
+          same += first >= 0 && first == prev;
+          prev = first;
+        }
+      }
+    }
     int c = -1, left = -1;
     if (valid) {
       if (prods[p].Ej) {  // the addend's entries count as products of the row
@@ -355,7 +385,11 @@ __global__ void __launch_bounds__(256) k_row_mults(
       c = sym_class(f, n, S->tune);
       // one-pass rows: their scratch bound; the class they leave is kept
       // (cand) in case the product takes the two-pass path after all
-      const bool one = S->onepass && onepass_row(f, n, S->tune);
+      // candidates: rows whose bound fits a warp's full table, and larger
+      // ones whose products look like repeating columns (their 64-slot
+      // attempt is likely to hold the row)
+      const bool one = S->onepass && onepass_row(f, n, S->tune) &&
+                       (onepass_full(f, n, S->tune) || (seen > 1 && 4 * same >= seen - 1));
       if (one) {
         left = c;
         c = CLS_ONEPASS;
@@ -458,7 +492,7 @@ __global__ void __launch_bounds__(256) k_scatter(
     r = g - base[p];
     if (MODE == 0) {
       c = sym_class(rowf[g], prods[p].n, S->tune);
-      if (S->onepass && onepass_row(rowf[g], prods[p].n, S->tune)) c = CLS_ONEPASS;
+      if (S->onepass && rowc[g] > 0) c = CLS_ONEPASS;  // the count pass's choice (bound > 0)
     } else {
       c = num_class(rowc[g], rowf[g], S->tune);
       const int64_t off = cp[g] - cp[base[p]];
