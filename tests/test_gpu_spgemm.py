@@ -275,6 +275,28 @@ def test_onepass_skips_rows_without_repeats(ctx):
     check_product(spgemm_poisoned(ctx, dA, dB), A, B)
 
 
+def test_onepass_without_workspace_budget():
+    # A context whose workspace budget (64 MB) holds the product's row arrays
+    # but not the one-pass workspace (~100 MB for the Galerkin A·P on 42^3):
+    # the product takes the two-pass path, same result
+    R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
+    c = ops.Context(0, budget=64 << 20)
+    try:
+        dA, dP = A.to_device(), P.to_device()
+        n0 = _launches(c)
+        C1 = ops.spgemm(c, dA, dP)
+        n1 = _launches(c)
+        plan = ops.Plan(c, dA, dP)
+        plan.numeric(dA, dP)
+        plan.close()
+        n2 = _launches(c)
+        assert (n1 - n0) - (n2 - n1) == 3  # the scan and the fold only
+        check_product(C1, A, P)
+    finally:
+        torch.cuda.synchronize()
+        c.close()
+
+
 def test_onepass_minority_folds_back(ctx):
     # R-MAT 17 A·A (131,072 rows): a tenth of the rows qualify for the
     # one-pass path, too few, so they go back to the warp class after their

@@ -85,6 +85,7 @@ struct tspg_plan {
     void *q = nullptr;
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 16;
+    if (nblocks == int(sizeof(blocks) / sizeof(blocks[0]))) return TSPG_ENOMEM;
     int st = ws_alloc(ctx, &q, bytes, stream);
     if (st != TSPG_OK) return st;
     blocks[nblocks++] = q;
