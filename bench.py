@@ -727,6 +727,15 @@ def run_rap(args):
     # the A·P rows are one-pass rows (multiplied whole in the first launch), so
     # the roofline takes both launches of the call
     ap_phases = ap_sym + ap_num
+    ap_traffic = (None, None)
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        ent = prof.get(f"rap27pt_{n}^3", {}).get(
+            "A·P, both launches (k_groups + k_onepass, then the copy of the one-pass rows)")
+        if ent:
+            ap_traffic = (int(ent["dram_bytes_per_launch"]), ent.get("source"))
+    except Exception:
+        pass
     # CPU baseline: the oracle on both products, repeated for at least ~5 s
     from trident_b200.synth import HostCSR
     reps, t0 = 0, time.perf_counter()
@@ -758,7 +767,8 @@ def run_rap(args):
         "roofline": {"bound": "hbm",
                      "kernel": "A·P, both launches (k_groups + k_onepass, then the copy of the one-pass rows)",
                      "achieved": round(bap / (ap_phases * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(bap / (ap_phases * 1e-3) / 1e9 / peak, 4), "traffic": None,
+                     "frac": round(bap / (ap_phases * 1e-3) / 1e9 / peak, 4), "traffic": ap_traffic[0],
+                     "traffic_source": ap_traffic[1],
                      "algorithmic_bytes": bap},
         "gpu_launches": int(l1.value - l0.value),
         "clocks": clk,
