@@ -222,10 +222,11 @@ int tspg_spgemm_row_products(tspg_ctx *ctx, void *stream, const tspg_csr *A,
  * Empty operands give an empty C with a zeroed rowptr (the num_prods == 0
  * exit, include/cusparse_helpers.cuh:1251-1257).  Synchronises `stream` once
  * (to learn nnz(C)); twice when A has at least 65,536 rows.  Such a product
- * whose rows are mostly warp rows (small product bounds) computes those rows
+ * whose rows are mostly short (or repeat their columns) computes those rows
  * whole in its first launch, into a workspace of 4 + val_bits / 8 bytes per
- * unit of their output bound (at most 2^30 units) taken from the context's
- * pool, and copies them into C in the second; when the budget refuses that
+ * entry they may write (at most 32 per row, or the row's bound when smaller;
+ * at most 2^30 entries) taken from the context's pool, and copies them into
+ * C in the second; when the budget refuses that
  * workspace, or the product has few such rows, every row takes the two-pass
  * path.  Results are the same either way; a plan (tspg_spgemm_symbolic)
  * always takes the two-pass path, since its numeric calls may bring new

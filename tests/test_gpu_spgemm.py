@@ -224,9 +224,9 @@ def _vstack(*Ms):
 
 def test_onepass_mixed_row_classes(ctx):
     # Most rows one-pass (Galerkin A·P on 42^3, ~12 columns each) beside rows
-    # whose first, 64-slot attempt is refused (40 random entries: ~150
-    # columns; redone with the full table) and rows of the 128-, 256- and
-    # CTA-thread classes (300 and 700 entries), into poisoned outputs
+    # of random entries that stay two-pass (40 entries: ~150 columns; 300 and
+    # 700 entries: 128-, 256- and CTA-thread rows) and short ones, into
+    # poisoned outputs
     R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
     rows = [A, random_csr(1500, A.ncols, per_row=40, seed=41), random_csr(300, A.ncols, per_row=300, seed=42),
             random_csr(100, A.ncols, per_row=700, seed=43), random_csr(500, A.ncols, per_row=2, seed=44)]
@@ -276,11 +276,11 @@ def test_onepass_skips_rows_without_repeats(ctx):
 
 
 def test_onepass_without_workspace_budget():
-    # A context whose workspace budget (64 MB) holds the product's row arrays
-    # but not the one-pass workspace (~100 MB for the Galerkin A·P on 42^3):
+    # A context whose workspace budget (16 MB) holds the product's row arrays
+    # but not the one-pass workspace (~28 MB for the Galerkin A·P on 42^3):
     # the product takes the two-pass path, same result
     R, A, P = workloads.galerkin_operands(n=42, pts=27, agg=3)
-    c = ops.Context(0, budget=64 << 20)
+    c = ops.Context(0, budget=16 << 20)
     try:
         dA, dP = A.to_device(), P.to_device()
         n0 = _launches(c)

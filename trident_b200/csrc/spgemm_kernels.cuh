@@ -93,19 +93,20 @@ __host__ __device__ inline int sym_class(int64_t f, int64_t n, const Tune &t) {
 // symbolic warp, 128- and 256-thread classes are multiplied whole by a warp
 // in the symbolic launch; their output waits in a scratch buffer for the
 // numeric launch, which copies it into C.  A row whose output bound
-// min(f, n) fits a warp's numeric table is always finished there; a larger
-// one is finished only when it has fewer than kCappedCols columns (its
-// 64-slot attempt), else it is deferred to the two-pass path.
+// min(f, n) fits a 64-slot table is always finished there; a larger one is
+// finished only when it has fewer than kCappedCols columns (its 64-slot
+// attempt), else it is deferred to the two-pass path — so no row writes
+// more than kCappedCols scratch entries, and the scratch stays dense.
 constexpr int kCappedCols = 32;
 __host__ __device__ inline bool onepass_row(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
   return f > 0 && fe <= t.sym[2];
 }
-// A one-pass row whose full table fits a warp (else only its 64-slot attempt
-// can finish it), and the scratch entries it may write.
+// A one-pass row whose whole table fits 64 slots (else only its capped
+// 64-slot attempt can finish it), and the scratch entries it may write.
 __host__ __device__ inline bool onepass_full(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
-  return int64_t(t.load) * fe <= kNumT32;
+  return int64_t(t.load) * fe <= 2 * kCappedCols;
 }
 __host__ __device__ inline int64_t onepass_bound(int64_t f, int64_t n, const Tune &t) {
   const int64_t fe = f < n ? f : n;
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(256) k_row_mults(
     {
       const int64_t fe = f < (valid ? prods[p].n : 0) ? f : (valid ? prods[p].n : 0);
       const bool need = S->onepass && valid && fe > 0 && fe <= S->tune.sym[2] &&
-                        int64_t(S->tune.load) * fe > kNumT32;
+                        int64_t(S->tune.load) * fe > 2 * kCappedCols;
       if (__any_sync(0xffffffffu, need)) {
         const int32_t *Bj = valid ? prods[p].Bj : nullptr;
         seen = need ? int(len < kHintEntries ? len : kHintEntries) : 0;

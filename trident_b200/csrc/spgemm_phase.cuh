@@ -673,10 +673,10 @@ __device__ __forceinline__ int warp_lean_output(const PhaseArgs &A, int *keys, c
 // m.off is the row's scratch offset; the row is written to the scratch
 // (A.oj / A.ox) with the count found here, which goes to rowc, and rowf
 // becomes -1 - offset (the numeric launch copies the row into C and skips it
-// otherwise).  A row whose bound min(products, ncols) is too large for a
-// warp's full table and which holds kCappedCols columns or more is instead
-// listed in A.defer for the two-pass path (its symbolic count follows in the
-// same launch).
+// otherwise).  A row whose bound min(products, ncols) needs more than 64
+// slots and which holds kCappedCols columns or more is instead listed in
+// A.defer for the two-pass path (its symbolic count follows in the same
+// launch sequence).
 template <int G, int TMAX, typename PT, typename VT, bool ONEPASS = false>
 __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                              const RowMeta &m, unsigned char *slice, const GroupMem &gm,
@@ -696,7 +696,6 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   int32_t *const oj = ONEPASS ? A.oj + off : P.Cj + off;
   VT *const ox = ONEPASS ? (VT *)A.ox + off : P.Cx + off;
   uint32_t Tfull = pow2_at_least(A.S->tune.load * c, 32);
-  const bool full_fits = Tfull <= TMAX;
   if (Tfull > TMAX) Tfull = TMAX;
   // Warp rows of at most 64 slots spread their values over NC copies of the
   // value table (lane & (NC - 1) picks one; copies 16 bytes apart in banks):
@@ -705,18 +704,17 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   // phase 3.72 ms with one table, 3.45 ms with 4 copies).
   constexpr int NC = G == 32 ? 4 : 1;
   static_assert(NC * (64 + 4) * 8 <= TMAX * 8, "value copies");
-  // A one-pass row whose bound needs more than 64 slots first tries 64 (its
-  // count is unknown; the Galerkin A·P rows bound ~119 and hold ~12): once
-  // 32 columns are in (a counter in the warp's list slot) no new column gets
-  // a slot, and a refused column sends the row to a second attempt with the
-  // full table.
+  // A one-pass row whose bound needs more than 64 slots tries 64 (its count
+  // is unknown; the Galerkin A·P rows bound ~119 and hold ~12): once 32
+  // columns are in (a counter in the warp's list slot) no new column gets a
+  // slot, and a refused column sends the row to the two-pass path.
   bool capped = ONEPASS && G == 32 && Tfull > 64;
   int *ocnt = gm.lst;  // warp rows: [0] admitted columns, [1] refused
   uint32_t T = Tfull;
   int logT = 0;
   uint32_t mask = 0;
   const int64_t a0 = m.a0, a1 = m.a1;
-  while (true) {
+  {  // the table, the products and (tables of at most 64 slots) the output
     T = capped ? 64 : Tfull;
     logT = ilog2_pow2(T);
     mask = T - 1;
@@ -752,17 +750,13 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
     if (capped) {
       const bool refused = ((volatile int *)ocnt)[1] != 0;
       __syncwarp();
-      if (refused) {
-        if (!full_fits) {  // too large for a warp: the two-pass path
-          if (lane == 0) {
-            const unsigned long long i = atomicAdd(&A.S->ndefer, 1ull);
-            A.defer[i] = (uint64_t(m.p) << 40) | uint64_t(m.r);
-          }
-          __syncwarp();
-          return;
+      if (refused) {  // 32 columns or more: the two-pass path
+        if (lane == 0) {
+          const unsigned long long i = atomicAdd(&A.S->ndefer, 1ull);
+          A.defer[i] = (uint64_t(m.p) << 40) | uint64_t(m.r);
         }
-        capped = false;  // again with the full table
-        continue;
+        __syncwarp();
+        return;
       }
     }
     if constexpr (G == 32) {
@@ -777,7 +771,6 @@ __device__ void num_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
         return;
       }
     }
-    break;
   }
   // In-place compaction into [0, c): targets lie in the first half (c <= T/2),
   // so first-half slots are held in registers across the group barrier inside
