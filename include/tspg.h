@@ -173,14 +173,14 @@ int tspg_ctx_get_tuning(const tspg_ctx *ctx, tspg_tuning *t);
 
 /* Per-class accounting of the persistent phases (off by default): SM cycles
  * and rows per row class, accumulated over calls since enabling.  out64 =
- * symbolic[32], numeric[32]; each half holds cycles x 7, rows x 7 (classes
+ * symbolic[32], numeric[32]; each half holds cycles x 8, rows x 8 (classes
  * DENSE0 (>= 2^20 products), DENSE1 (>= 2^17), DENSE2, G1024, G256, G128,
- * G32), then sub-phase cycles: [14..18] the whole-row DENSE rows' bitmap
- * pass, block scan, zero fill, column emission and value pass; [19..22] the
- * windowed DENSE rows' set-up, short-entry walks, long-entry walks and
- * emission; [23..27] the group rows' set-up, products, compaction, sort and
- * write (symbolic: set-up, products, count).  Reading synchronises the
- * device. */
+ * G32, then the one-pass warp rows, counted in the symbolic half), then
+ * sub-phase cycles: [16..20] the whole-row DENSE rows' bitmap pass, block
+ * scan, zero fill, column emission and value pass; [21..24] the windowed
+ * DENSE rows' set-up, short-entry walks, long-entry walks and emission;
+ * [25..29] the group rows' set-up, products, compaction, sort and write
+ * (symbolic: set-up, products, count).  Reading synchronises the device. */
 int tspg_ctx_class_profile(tspg_ctx *ctx, int enable);
 int tspg_ctx_class_cycles(tspg_ctx *ctx, uint64_t *out64);
 

@@ -346,7 +346,7 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
       PhaseArgs pa{b->d_base, b->sched, b->list, b->rowf, b->rowc, b->cp, nullptr, 0, errw,
                    ctx->d_prof};
       phase_mark(ctx, 0, 0, s);
-      k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+      k_phase<PT, VT, false><<<ctx->num_sms, kSymThreads, kDynSmem, s>>>(prods, pa);
       k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 0, 1, s);
       k_scan_reduce<<<(unsigned)nb, kScanThreads, 0, s>>>(b->rowc, R, b->partial);

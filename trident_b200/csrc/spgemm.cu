@@ -205,7 +205,7 @@ static int symbolic_impl(tspg_ctx *ctx, cudaStream_t s, const tspg_csr *A,
     pa.ox = P->ox;
     pa.defer = P->defer;
     phase_mark(ctx, 0, 0, s);
-    k_phase<PT, VT, false><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
+    k_phase<PT, VT, false><<<ctx->num_sms, kSymThreads, kDynSmem, s>>>(prods, pa);
     k_groups<PT, VT, false><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
     if (onepass) {
       k_onepass<PT, VT><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);

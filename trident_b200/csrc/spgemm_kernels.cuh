@@ -32,6 +32,9 @@
 namespace tspg {
 
 constexpr int kThreads = 512;   // persistent CTA: 16 warps x 128 registers
+// The symbolic CTA rows need no values (80 registers), so their persistent
+// CTA runs 24 warps: more B-row loads and bitmap updates in flight per SM.
+constexpr int kSymThreads = 768;
 constexpr int kTableSmem = 196608;              // hash tables / dense window
 constexpr int kCountSmem = 16384;               // radix-sort digit counters
 constexpr int kDynSmem = kTableSmem + kCountSmem;  // one CTA per SM

@@ -21,18 +21,20 @@ namespace tspg {
 
 // Walk B entries q0, q0 + step, ... below b1 calling fn(col, a*b), with U
 // loads in flight per thread (all loads of a step are issued before the
-// updates, so the L2/HBM latency is paid once per U entries).
-template <bool NUM, typename VT, typename F>
+// updates, so the L2/HBM latency is paid once per U entries).  IX is the
+// position type: uint32_t when B's row offsets are 32-bit (positions below
+// 2^31, so q + U * step stays below 2^32 for step <= 2^27), else int64_t.
+template <bool NUM, typename IX, typename VT, typename F>
 __device__ __forceinline__ void walk_row(const int32_t *__restrict__ Bj,
-                                         const VT *__restrict__ Bx, int64_t q0,
-                                         int64_t b1, int step, VT a, F &&fn) {
+                                         const VT *__restrict__ Bx, IX q0, IX b1, int step,
+                                         VT a, F &&fn) {
   constexpr int U = 8;
-  for (int64_t q = q0; q < b1; q += int64_t(step) * U) {
+  for (IX q = q0; q < b1; q += IX(step) * U) {
     int32_t c[U];
     VT x[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      const int64_t qq = q + int64_t(u) * step;
+      const IX qq = q + IX(u) * IX(step);
       c[u] = qq < b1 ? __ldg(Bj + qq) : -1;
       if constexpr (NUM) x[u] = qq < b1 ? __ldg(Bx + qq) : VT(0);
     }
@@ -62,6 +64,7 @@ __device__ __forceinline__ void for_products_balanced(
     const PT *__restrict__ Bp, const int32_t *__restrict__ Bj,
     const VT *__restrict__ Bx, int64_t a0, int64_t a1, int64_t f, int S,
     int lane, int gid, int *lst, int *nl, int cap, F &&fn, int *ctr = nullptr) {
+  using IX = std::conditional_t<sizeof(PT) == 4, uint32_t, int64_t>;
   const int sub = lane / S, sl = lane - sub * S, nsub = G / S;
   const int64_t thr = nsub > 1 ? max(int64_t(4 * S), f / nsub) : INT64_MAX;
   const unsigned submask =
@@ -81,8 +84,8 @@ __device__ __forceinline__ void for_products_balanced(
       p += nsub;
     }
     const int64_t k = __ldg(Aj + pc);
-    const int64_t b0 = __ldg(Bp + k), b1 = __ldg(Bp + k + 1);
-    if (b1 - b0 > thr) {
+    const IX b0 = IX(__ldg(Bp + k)), b1 = IX(__ldg(Bp + k + 1));
+    if (int64_t(b1 - b0) > thr) {
       int slot = 0;
       if (sl == 0) slot = atomicAdd(nl, 1);
       slot = __shfl_sync(submask, slot, (lane & 31) - sl);
@@ -93,7 +96,7 @@ __device__ __forceinline__ void for_products_balanced(
     }
     VT a = VT(0);
     if constexpr (NUM) a = __ldg(Ax + pc);
-    walk_row<NUM, VT>(Bj, Bx, b0 + sl, b1, S, a, fn);
+    walk_row<NUM, IX, VT>(Bj, Bx, b0 + IX(sl), b1, S, a, fn);
   }
   group_sync<G>(gid);
   const int n = min(*nl, cap);
@@ -102,7 +105,8 @@ __device__ __forceinline__ void for_products_balanced(
     const int64_t k = __ldg(Aj + p);
     VT a = VT(0);
     if constexpr (NUM) a = __ldg(Ax + p);
-    walk_row<NUM, VT>(Bj, Bx, __ldg(Bp + k) + lane, __ldg(Bp + k + 1), G, a, fn);
+    walk_row<NUM, IX, VT>(Bj, Bx, IX(__ldg(Bp + k)) + IX(lane), IX(__ldg(Bp + k + 1)), G, a,
+                          fn);
   }
 }
 
@@ -466,7 +470,7 @@ __device__ void sym_hash_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   prof_sub_g(A, 11, tp, lane == 0);
 }
 
-template <typename PT, typename VT>
+template <int NT, typename PT, typename VT>
 __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                               int64_t idx, unsigned char *smem, const GroupMem &gm) {
   int64_t *scan_tmp = gm.tmp;
@@ -482,23 +486,25 @@ __device__ void sym_dense_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
   for (int64_t w0 = 0; w0 < n; w0 += W) {
     const int64_t w1 = (w0 + W < n) ? w0 + W : n;
     const int64_t nw = (w1 - w0 + 31) >> 5;
-    for (int64_t i = tid; i < nw; i += kThreads) bm[i] = 0u;
+    for (int64_t i = tid; i < nw; i += NT) bm[i] = 0u;
     __syncthreads();
+    // columns are below 2^31: one unsigned compare tests w0 <= col < w1
+    const uint32_t uw0 = uint32_t(w0), uW = uint32_t(w1 - w0);
     auto mark = [&](int32_t col, VT) {
-      if (col >= w0 && col < w1) {
-        const uint32_t o = uint32_t(col - w0);
+      const uint32_t o = uint32_t(col) - uw0;
+      if (o < uW) {
         const uint32_t bit = 1u << (o & 31);
         if (!(((volatile uint32_t *)bm)[o >> 5] & bit)) atomicOr(bm + (o >> 5), bit);
       }
     };
-    for_products_balanced<kThreads, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
-                                                   A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl,
-                                                   gm.cap, mark, gm.nl - 1);
-    for_addend<false>(P, rr.r, tid, kThreads, mark);
+    for_products_balanced<NT, false, PT, VT>(P.Aj, P.Ax, P.Bp, P.Bj, P.Bx, a0, a1,
+                                             A.rowf[rr.g], S, tid, 0, gm.lst, gm.nl, gm.cap,
+                                             mark, gm.nl - 1);
+    for_addend<false>(P, rr.r, tid, NT, mark);
     __syncthreads();
     int64_t local = 0;
-    for (int64_t i = tid; i < nw; i += kThreads) local += __popc(bm[i]);
-    total += group_sum<kThreads, int64_t>(local, scan_tmp, 0);
+    for (int64_t i = tid; i < nw; i += NT) local += __popc(bm[i]);
+    total += group_sum<NT, int64_t>(local, scan_tmp, 0);
   }
   if (tid == 0) A.rowc[rr.g] = int32_t(total);
 }
@@ -1749,8 +1755,9 @@ __device__ void group_rows(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
 }
 
 template <typename PT, typename VT, bool NUM>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(NUM ? kThreads : kSymThreads, 1)
     k_phase(const ProdDev<PT, VT> *prods, PhaseArgs A) {
+  constexpr int NT = NUM ? kThreads : kSymThreads;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ PhaseShared sh;
   __shared__ int64_t s_items[kCtaClasses + 1];
@@ -1812,15 +1819,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         else
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);
       } else {
-        sym_dense_row<PT, VT>(prods, A, idx, smem, gm);
+        sym_dense_row<NT, PT, VT>(prods, A, idx, smem, gm);
       }
     } else {
       if constexpr (NUM)
         num_hash_row<kThreads, kNumT1024, PT, VT>(prods, A, load_meta<true>(prods, A, idx), smem,
                                                   gm, 0, tid);
       else
-        sym_hash_row<kThreads, kSymT1024, PT, VT>(prods, A, load_meta<false>(prods, A, idx),
-                                                  (int *)smem, gm, 0, tid);
+        sym_hash_row<NT, kSymT1024, PT, VT>(prods, A, load_meta<false>(prods, A, idx),
+                                            (int *)smem, gm, 0, tid);
     }
     prof_add(A, c, t0, tid == 0);
     __syncthreads();
