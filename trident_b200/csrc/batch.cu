@@ -221,6 +221,8 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_phase<PT, VT, true>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
+  TSPG_CUDA(ctx, cudaFuncSetAttribute(k_dense_rank<PT, VT>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, kDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_groups<PT, VT, false>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kGroupDynSmem));
   TSPG_CUDA(ctx, cudaFuncSetAttribute(k_groups<PT, VT, true>,
@@ -422,12 +424,13 @@ static int batch_run_impl(tspg_batch *b, cudaStream_t s, int flags) {
                    b->curbuf, b->cur_stride, errw, ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
       phase_mark(ctx, 1, 0, s);
       launch_dense_cluster<PT, VT>(ctx, s, prods, pa);  // launchable: checked above
+      k_dense_rank<PT, VT><<<ctx->num_sms, kRankThreads, kDynSmem, s>>>(prods, pa);
       k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
       k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
       phase_mark(ctx, 1, 1, s);
     }
     k_zero_rowptr<PT, VT><<<(nprod + 31) / 32, 32, 0, s>>>(prods, nprod);
-    b->g2_kernels = 2 + (R > 0 ? 4 + (ctx->tune.cluster ? 1 : 0) : 0);
+    b->g2_kernels = 2 + (R > 0 ? 5 + (ctx->tune.cluster ? 1 : 0) : 0);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (e != cudaSuccess) {
       ctx->last_cuda = (int)e;

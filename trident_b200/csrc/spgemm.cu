@@ -39,8 +39,11 @@ static int set_smem_attr(int device) {
     cudaError_t e5 = cudaFuncSetAttribute(k_onepass<PT, VT>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kGroupDynSmem);
+    cudaError_t e6 = cudaFuncSetAttribute(k_dense_rank<PT, VT>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kDynSmem);
     if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess ||
-        e5 != cudaSuccess)
+        e5 != cudaSuccess || e6 != cudaSuccess)
       return TSPG_ECUDA;
     if (cached) done[device] = true;
   }
@@ -272,13 +275,14 @@ static int numeric_impl(tspg_ctx *ctx, cudaStream_t s, tspg_plan *P,
                ctx->d_prof ? ctx->d_prof + kProfPerPhase : nullptr};
   phase_mark(ctx, 1, 0, s);
   TSPG_CUDA(ctx, launch_dense_cluster<PT, VT>(ctx, s, prods, pa));
+  k_dense_rank<PT, VT><<<ctx->num_sms, kRankThreads, kDynSmem, s>>>(prods, pa);
   k_phase<PT, VT, true><<<ctx->num_sms, kThreads, kDynSmem, s>>>(prods, pa);
   k_groups<PT, VT, true><<<ctx->num_sms, kGroupThreads, kGroupDynSmem, s>>>(prods, pa);
   if (P->onepass)
     k_onepass_copy<PT, VT><<<grid_for(m * 32, 256, ctx->num_sms * 16), 256, 0, s>>>(
         prods, P->rowf, P->rowc, P->cp, P->oj, (const VT *)P->ox, m);
   phase_mark(ctx, 1, 1, s);
-  ctx->launches += 5 + (P->onepass ? 1 : 0);
+  ctx->launches += 6 + (P->onepass ? 1 : 0);
   TSPG_CUDA(ctx, cudaGetLastError());
   return TSPG_OK;
 }

@@ -1082,7 +1082,7 @@ __device__ void num_esc_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A, co
 // by entries, not by words (R-MAT bitmaps are far denser at the hub columns);
 // pass 2 adds every product into its output slot, found as base + popc of the
 // bits below, with a fire-and-forget global FP64 reduction.  No sort.
-template <typename PT, typename VT>
+template <int NT, typename PT, typename VT>
 __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs &A,
                                    int64_t idx, unsigned char *smem, const GroupMem &gm) {
   const int tid = threadIdx.x;
@@ -1107,16 +1107,16 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   const VT *__restrict__ Bx = P.Bx;
   const int S1 = subgroup_width_avg(f, na, 32);
   long long tp = clock64();
-  for (int i = tid; i < nb * 32; i += kThreads) bm[i] = 0u;
+  for (int i = tid; i < nb * 32; i += NT) bm[i] = 0u;
   __syncthreads();
   auto mark = [&](int32_t col, VT) {
     const uint32_t bit = 1u << (col & 31);
     uint32_t &x = bmw(col >> 5);
     if (!(*(volatile uint32_t *)&x & bit)) atomicOr(&x, bit);
   };
-  for_products_balanced<kThreads, false, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
+  for_products_balanced<NT, false, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
                                                  gm.lst, gm.nl, gm.cap, mark, gm.nl - 1);
-  for_addend<false>(P, rr.r, tid, kThreads, mark);
+  for_addend<false>(P, rr.r, tid, NT, mark);
   __syncthreads();
   prof_sub(A, 0, tp);
   // Block scan: block b = words [32b, 32b + 32), lane l of a warp takes word
@@ -1126,7 +1126,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     const int warp = tid >> 5, lane = tid & 31;
     // four blocks per step: their scans are independent, so their shuffle
     // latencies overlap
-    constexpr int NW = kThreads / 32, UB = 4;
+    constexpr int NW = NT / 32, UB = 4;
     for (int b0 = warp; b0 < nb; b0 += NW * UB) {
       int pc[UB], inc[UB];
 #pragma unroll
@@ -1148,7 +1148,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   }
   __syncthreads();
   {
-    constexpr int BPT = 3;  // blocks per thread: nb <= kRankMaxCols / 1024 < 3 * kThreads
+    constexpr int BPT = 3;  // blocks per thread: nb <= kRankMaxCols / 1024 < 3 * NT
     int v[BPT], sum = 0;
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
@@ -1158,7 +1158,7 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     }
     int64_t tot;
     // the scan ends on a barrier, so every read of bbase above is done
-    int run = int(group_excl_scan<kThreads, int64_t>(int64_t(sum), gm.tmp, 0, &tot));
+    int run = int(group_excl_scan<NT, int64_t>(int64_t(sum), gm.tmp, 0, &tot));
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
       const int b = tid * BPT + k;
@@ -1175,18 +1175,18 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   // zeroed values: a contiguous range, coalesced
   // the values stay in L2 for the reductions, the indices may leave first
   const uint64_t keep = policy_evict_last(), pass = policy_evict_first();
-  for (int64_t e = tid; e < c; e += kThreads) store_hint(Cx + e, VT(0), keep);
+  for (int64_t e = tid; e < c; e += NT) store_hint(Cx + e, VT(0), keep);
   prof_sub(A, 2, tp);
   // Column indices.  The bitmap walk is a merge of two sequences, the words
   // and the set bits (nw + c steps: every bit, then a step to the next word);
-  // thread t takes steps [d_t, d_t+1), d_t = t * (nw + c) / kThreads (merge-
+  // thread t takes steps [d_t, d_t+1), d_t = t * (nw + c) / NT (merge-
   // path split), so threads get equal work however the bits cluster, and the
   // loop below takes exactly one step per iteration, so the lanes of a warp
   // stay in step.  A split point is found by searching w + rank(w) over the
   // block bases, then over the word offsets of one block.
   {
     const int64_t steps = int64_t(nw) + c;
-    const int64_t d0 = steps * tid / kThreads, d1 = steps * (tid + 1) / kThreads;
+    const int64_t d0 = steps * tid / NT, d1 = steps * (tid + 1) / NT;
     int lo = 0, hi = nb - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -1228,9 +1228,9 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
     return bbase[w >> 5] + int(wp[w]) + __popc(bmw(w) & ((1u << (col & 31)) - 1u));
   };
   auto put = [&](int32_t col, VT v) { red_add_hint(Cx + rank_of(col), v, keep); };
-  for_products_balanced<kThreads, true, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
+  for_products_balanced<NT, true, PT, VT>(Aj, Ax, Bp, Bj, Bx, a0, a1, f, S1, tid, 0,
                                                 gm.lst, gm.nl, gm.cap, put, gm.nl - 1);
-  for_addend<true>(P, rr.r, tid, kThreads, put);
+  for_addend<true>(P, rr.r, tid, NT, put);
   __syncthreads();
   prof_sub(A, 4, tp);
 }
@@ -1783,11 +1783,13 @@ __global__ void __launch_bounds__(NUM ? kThreads : kSymThreads, 1)
   gm.nl = sh.nl + 47;
   gm.cap = 1024;
   gm.stage = nullptr;
+  // numeric: when k_dense_rank did every DENSE row, start past them
+  const int64_t first = NUM && A.S->rank_left == 0 ? s_items[CLS_DENSE2 + 1] : 0;
   // stage 1: CTA-level rows, heaviest class first
   while (true) {
     if (tid == 0) sh.slot[15] = atomicAdd(&A.S->work, 1ull);
     __syncthreads();
-    const int64_t item = (int64_t)sh.slot[15];
+    const int64_t item = first + (int64_t)sh.slot[15];
     __syncthreads();
     if (item >= s_items[kCtaClasses]) break;
     // numeric: the heavy DENSE0 / DENSE1 rows (heaviest first) are interleaved
@@ -1795,7 +1797,7 @@ __global__ void __launch_bounds__(NUM ? kThreads : kSymThreads, 1)
     // in flight at once and their output segments (the targets of the global
     // reductions) stay in L2; symbolic: heaviest first
     int64_t pos = item;
-    if (NUM) {
+    if (NUM && first == 0) {
       const int64_t H = s_items[2], L = s_items[kCtaClasses] - H;
       int64_t K = H > 0 ? min(int64_t(kHeavyPeriod), 1 + L / H) : 1;
       // (past the interleaved stretch the light rows follow in order: pos = item)
@@ -1814,10 +1816,9 @@ __global__ void __launch_bounds__(NUM ? kThreads : kSymThreads, 1)
         // that ran before this one
         if (win_row(P, A.rowf[rr.g], int64_t(A.rowc[rr.g]), A.S->tune)) {
           if (A.S->tune.cluster == 0) num_dense_win_row<PT, VT>(prods, A, idx, smem, gm);
-        } else if (P.n <= kRankMaxCols)
-          num_dense_rank_row<PT, VT>(prods, A, idx, smem, gm);
-        else
+        } else if (P.n > kRankMaxCols) {
           num_dense_row<PT, VT>(prods, A, idx, smem, gm);
+        }  // else: a rank-form row, done by k_dense_rank before this kernel
       } else {
         sym_dense_row<NT, PT, VT>(prods, A, idx, smem, gm);
       }
@@ -1830,6 +1831,54 @@ __global__ void __launch_bounds__(NUM ? kThreads : kSymThreads, 1)
                                             (int *)smem, gm, 0, tid);
     }
     prof_add(A, c, t0, tid == 0);
+    __syncthreads();
+  }
+}
+
+// The numeric DENSE rows of the rank form (at most kRankMaxCols columns, not
+// taken by the column-window rule), persistent, before k_phase: 24 warps per
+// SM, where k_phase's 16 warps keep the 128 registers of the hash rows'
+// radix sort.  Heavy rows (DENSE0 / DENSE1) are spread over the DENSE2 rows
+// as in k_phase, so few of their reduction targets are live at once.
+template <typename PT, typename VT>
+__global__ void __launch_bounds__(kRankThreads, 1)
+    k_dense_rank(const ProdDev<PT, VT> *prods, PhaseArgs A) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ PhaseShared sh;
+  __shared__ unsigned long long s_item;
+  const int tid = threadIdx.x;
+  const int64_t H = A.S->cnt[CLS_DENSE0] + A.S->cnt[CLS_DENSE1];
+  const int64_t L = A.S->cnt[CLS_DENSE2];
+  const int64_t c01 = A.S->cnt[CLS_DENSE0];
+  const int64_t K = H > 0 ? min(int64_t(kHeavyPeriod), 1 + L / H) : 1;
+  GroupMem gm;
+  gm.cnt = nullptr;
+  gm.tmp = sh.scan;
+  gm.itmp = sh.itmp;
+  gm.lst = sh.lst;
+  gm.nl = sh.nl + 47;
+  gm.cap = 1024;
+  gm.stage = nullptr;
+  while (true) {
+    if (tid == 0) s_item = atomicAdd(&A.S->work3, 1ull);
+    __syncthreads();
+    const int64_t item = (int64_t)s_item;
+    __syncthreads();
+    if (item >= H + L) break;
+    int64_t pos = item;
+    if (K > 1 && item < K * H) pos = item % K == 0 ? item / K : H + (item - item / K - 1);
+    // the DENSE classes' lists are contiguous: DENSE0, DENSE1, DENSE2
+    const int c = pos < c01 ? CLS_DENSE0 : pos < H ? CLS_DENSE1 : CLS_DENSE2;
+    const int64_t idx = A.S->off[CLS_DENSE0] + pos;
+    const long long t0 = clock64();
+    const RowRef rr = decode_row(A, idx);
+    const ProdDev<PT, VT> &P = prods[rr.p];
+    if (P.n <= kRankMaxCols && !win_row(P, A.rowf[rr.g], int64_t(A.rowc[rr.g]), A.S->tune)) {
+      num_dense_rank_row<kRankThreads, PT, VT>(prods, A, idx, smem, gm);
+      prof_add(A, c, t0, tid == 0);
+    } else if (tid == 0) {
+      A.S->rank_left = 1;  // read by k_phase, which runs after this kernel
+    }
     __syncthreads();
   }
 }
