@@ -349,7 +349,7 @@ def run_ours(args, rank, world):
     bytes_c = csr_bytes(pm, nnz_c, rp_bits // 8)
     algo = bytes_p + bytes_a + bytes_c
     sym, num = statistics.mean(sym_ms), statistics.mean(num_ms)
-    dom_ms, dom_name = ((num, "numeric phase (k_phase + k_groups)") if num >= sym
+    dom_ms, dom_name = ((num, "numeric phase (k_dense_rank + k_phase + k_groups)") if num >= sym
                         else (sym, "symbolic phase (k_phase + k_groups)"))
     try:
         peak, peak_src = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
