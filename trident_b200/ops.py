@@ -24,17 +24,27 @@ def _stream_ptr(stream=None) -> int:
 
 
 class _TorchAlloc:
-    """Allocator callback handing torch tensors to the library (kept alive here)."""
+    """Allocator callback handing torch tensors to the library (kept alive here).
+
+    The callback never raises: an exception inside a ctypes callback is
+    printed and the C caller receives an undefined pointer, so a failed
+    allocation returns NULL instead, which the library reports as
+    TSPG_ENOMEM.  The callback closes over the tensor list, not over this
+    object, so no reference cycle keeps the outputs alive after the call."""
 
     def __init__(self, device):
         self.device = device
-        self.tensors = []
-        self.cb = ALLOC_FN(self._alloc)
+        tensors = self.tensors = []
 
-    def _alloc(self, user, nbytes, stream):
-        t = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=self.device)
-        self.tensors.append(t)
-        return t.data_ptr()
+        def _alloc(user, nbytes, stream):
+            try:
+                t = torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=device)
+            except Exception:  # out of device memory: NULL -> TSPG_ENOMEM
+                return None
+            tensors.append(t)
+            return t.data_ptr()
+
+        self.cb = ALLOC_FN(_alloc)
 
 
 class Context:
@@ -195,6 +205,8 @@ def _finish(o: TspgCsrOut, rp, alloc: _TorchAlloc, val_bits: int) -> DeviceCSR:
         col = torch.empty(1, dtype=torch.int32, device=rp.device)
         val = torch.empty(1, dtype=_vdtype(val_bits), device=rp.device)
         return DeviceCSR(int(o.nrows), int(o.ncols), rp, col, val, nnz=0)
+    if len(alloc.tensors) < 2:
+        raise TspgError(TSPG_ENOMEM, "output allocation")
     colbuf, valbuf = alloc.tensors[-2], alloc.tensors[-1]
     col = colbuf.view(torch.int32)[:nnz]
     val = valbuf.view(_vdtype(val_bits))[:nnz]

@@ -29,8 +29,8 @@ import time
 # class (the defaults), and bounds stay non-decreasing over the classes.
 SYM_CAP = [512, 2048, 4096, 24576]
 NUM_CAP = [256, 1024, 2048, 8192]
-SYM_CHOICES = [[128, 256, 512], [1024, 2048], [2048, 3072, 4096], [8192, 12288, 24576]]
-NUM_CHOICES = [[128, 192, 256], [512, 768, 1024], [1024, 1536, 2048], [4096, 6144, 8192]]
+SYM_CHOICES = [[128, 256, 512], [1024, 2048], [2048, 3072, 4096], [4096, 6144, 8192, 12288, 24576]]
+NUM_CHOICES = [[128, 192, 256], [512, 768, 1024], [1024, 1536, 2048], [2048, 3072, 4096, 6144, 8192]]
 LOAD_CHOICES = [2, 4]
 # DENSE numeric rows with >= 2^w products (and an output filling >= 1/16 of the
 # columns) take the column-window form; 0 = never
