@@ -58,3 +58,40 @@ def test_batch_recaptures_on_tuning_change(tctx):
     for i, (A, B) in enumerate(hosts):
         check_product(b.result(i), A, B)
     b.close()
+
+
+@pytest.mark.parametrize("t", TUNINGS[1:])
+def test_batch_results_do_not_depend_on_tuning(tctx, t):
+    """Products of different shapes in one batch, with most rows (or all) in
+    the DENSE forms: the rank-form kernel takes rows of several products,
+    each with its own column count."""
+    tctx.set_tuning(t)
+    specs = workloads.batched_specs(count=5, seed=21, rows_lo=200, rows_hi=5000)
+    hosts, keep = [], []
+    b = ops.Batch(tctx)
+    for spec in specs:
+        A, B = workloads.batched_product(spec)
+        dA, dB = A.to_device(), B.to_device()
+        hosts.append((A, B))
+        keep.append((dA, dB))
+        b.add(dA, dB)
+    b.run()
+    for i, (A, B) in enumerate(hosts):
+        check_product(b.result(i), A, B)
+    b.close()
+
+
+def test_plan_numeric_with_dense_rows(tctx):
+    """The plan API's numeric re-runs (new values, same structure) with every
+    row above 256 outputs in the DENSE forms."""
+    tctx.set_tuning(TUNINGS[1])
+    R = workloads.rmat(scale=12, edge_factor=16, seed=5)
+    dR = R.to_device()
+    plan = ops.Plan(tctx, dR, dR)
+    try:
+        check_product(plan.numeric(dR, dR), R, R)
+        R.val[:] = R.val * -0.5 + 0.25
+        dR2 = R.to_device()
+        check_product(plan.numeric(dR2, dR2), R, R)
+    finally:
+        plan.close()
