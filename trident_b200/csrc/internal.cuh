@@ -301,6 +301,11 @@ __device__ __forceinline__ void store_hint(float *p, float v, uint64_t pol) {
 __device__ __forceinline__ void store_hint(int32_t *p, int32_t v, uint64_t pol) {
   asm volatile("st.global.L2::cache_hint.b32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(pol) : "memory");
 }
+// 16 zero bytes at a 16-byte aligned address
+__device__ __forceinline__ void store_zero16(void *p, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.b32 [%0], {%1, %1, %1, %1}, %2;" ::"l"(p), "r"(0),
+               "l"(pol) : "memory");
+}
 __device__ __forceinline__ void red_add(float *p, float v) {
   asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }

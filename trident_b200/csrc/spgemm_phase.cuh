@@ -1175,7 +1175,18 @@ __device__ void num_dense_rank_row(const ProdDev<PT, VT> *prods, const PhaseArgs
   // zeroed values: a contiguous range, coalesced
   // the values stay in L2 for the reductions, the indices may leave first
   const uint64_t keep = policy_evict_last(), pass = policy_evict_first();
-  for (int64_t e = tid; e < c; e += NT) store_hint(Cx + e, VT(0), keep);
+  {
+    // 16-byte stores from the first 16-byte boundary, scalar head and tail
+    const int64_t bytes = c * int64_t(sizeof(VT));
+    const int64_t head = min(bytes, int64_t((16 - (reinterpret_cast<uintptr_t>(Cx) & 15)) & 15));
+    const int64_t hn = head / int64_t(sizeof(VT));
+    const int64_t nv = (bytes - head) >> 4;
+    const int64_t t0 = hn + nv * int64_t(16 / sizeof(VT));
+    unsigned char *const zb = reinterpret_cast<unsigned char *>(Cx) + head;
+    for (int64_t e = tid; e < hn; e += NT) store_hint(Cx + e, VT(0), keep);
+    for (int64_t v = tid; v < nv; v += NT) store_zero16(zb + (v << 4), keep);
+    for (int64_t e = t0 + tid; e < c; e += NT) store_hint(Cx + e, VT(0), keep);
+  }
   prof_sub(A, 2, tp);
   // Column indices.  The bitmap walk is a merge of two sequences, the words
   // and the set bits (nw + c steps: every bit, then a step to the next word);
